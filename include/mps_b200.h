@@ -1,0 +1,254 @@
+/*
+ * mps_b200.h -- C-ABI of the B200-native explicit MPS solver.
+ *
+ * This is the drop-in boundary for the explicit MPS time step of frsykzk/MPS_CUDA.
+ * The reference exposes its solver only as `class MPS` (class.cuh:5-144): argument-less
+ * methods operating on public members, device buffers allocated with cudaMalloc, errors
+ * reported through `CHECK` -> exit(1) (const.cuh:87-95). This header replaces that
+ * surface with a handle-based C-ABI: plain pointers and sizes, every call returns an
+ * `int` status code (MPS_OK on success), nothing calls exit().
+ *
+ * Layout conventions
+ *  - Particle arrays are indexed by particle id (the input order, = the reference's
+ *    index `i` after RdDat, kernel.cu:110-131). Vectors are SoA: a `pos` buffer holds
+ *    x[0..n), y[0..n), z[0..n) back to back (the reference's areal3, const.cuh:67-71).
+ *  - `real` buffers are float for MPS_F32 / MPS_F32_N64 handles and double for MPS_F64.
+ *  - Wall normals are the reference's WLLVec: unit vectors pointing INTO the fluid
+ *    (RdDat negates the file normal, kernel.cu:127-128).
+ *  - Host buffers are only borrowed for the duration of a call; device buffers are owned
+ *    by the handle.
+ *  - A handle is not thread-safe: use one handle per host thread. Work is queued on the
+ *    handle's stream (mps_set_stream); calls that return host data synchronise it.
+ */
+#ifndef MPS_B200_H
+#define MPS_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (replace CHECK -> exit(1), const.cuh:87-95) ---------------------- */
+enum {
+    MPS_OK = 0,
+    MPS_ERR_ARG = 1,         /* invalid argument / inconsistent sizes                 */
+    MPS_ERR_CUDA = 2,        /* a CUDA runtime call failed (see mps_last_error)        */
+    MPS_ERR_NOMEM = 3,       /* device or host allocation failed                       */
+    MPS_ERR_STATE = 4,       /* call not valid in the handle's current state           */
+    MPS_ERR_OVERFLOW = 5,    /* a fixed capacity was exceeded (mirror slots, scratch)  */
+    MPS_ERR_TIMEOUT = 6,     /* a bounded device-side wait ran out                     */
+    MPS_ERR_UNSUPPORTED = 7, /* option not available in this build                     */
+    MPS_ERR_NODEVICE = 8     /* no CUDA device                                         */
+};
+
+/* ---- particle types (const.cuh:28-33) and wall flags (const.cuh:35-36) -------------- */
+enum { MPS_GST = -1, MPS_FLD = 0, MPS_WLL = 1, MPS_OBJ = 2, MPS_OBJ2 = 3, MPS_MRR = 4 };
+enum { MPS_SURFACE = 0, MPS_EDGE = 1 };
+
+/* maximum mirror particles generated from one fluid particle (const.cuh:50) */
+#define MPS_NUM_MRR 10
+
+/* ---- arithmetic of a handle (`typedef float real`, const.cuh:52-53) ----------------- */
+enum {
+    MPS_F32 = 0,     /* float state, float number density (the reference's typedef)  */
+    MPS_F64 = 1,     /* double state (the commented `typedef double real`)            */
+    MPS_F32_N64 = 2  /* float state, number density accumulated in double             */
+};
+
+/*
+ * Physical parameters of one scene. Mirrors MPS_physical.txt (kernel.cu:12-22) plus the
+ * values SetPara derives from it (kernel.cu:398-415) that are taken explicitly here:
+ *  - `snd`, `dt`, `umax`, `pmax` are inputs. SetPara derives them from the fluid height
+ *    along y and G.y (kernel.cu:399-415), which is degenerate when gravity points along z
+ *    (umax = 0, dt = inf, Pmax = 0). mps_params_dambreak() fills them with
+ *    umax = sqrt(2|g|H), pmax = rho |g| H for H the fluid height along gravity.
+ *  - Prs_coef = snd^2 / n0_grad (kernel.cu:409) and every lattice constant are derived
+ *    inside the library exactly as SetPara does (kernel.cu:336-373).
+ */
+typedef struct mps_params {
+    double pcl_dst;      /* PCL_DST: particle spacing l0 [m]                    (item 17) */
+    double min[3];       /* domain minimum before the 3.1*l0 padding            (items 1-3) */
+    double max[3];       /* domain maximum before the 3.1*l0 padding            (items 4-6) */
+    double g[3];         /* gravity G [m/s^2]                                   (items 7-9) */
+    double knm_vsc;      /* KNM_VSC: kinematic viscosity [m^2/s]                (item 16) */
+    double col_rat;      /* COL_RAT: collision restitution, COL = 1 + COL_RAT   (item 14) */
+    double dst_lmt_rat;  /* DST_LMT_RAT: rlim = DST_LMT_RAT * l0                (item 15) */
+    double rho;          /* particle density Dns of every type (const.cuh:38-41, kernel.cu:379-383) */
+    double snd;          /* SND: sound speed [m/s]                                        */
+    double dt;           /* time step [s]                                                 */
+    double umax;         /* speed clamp in ChkPcl (kernel.cu:493)                          */
+    double pmax;         /* pressure clamp in MkPrs (kernel.cu:1398)                       */
+    int32_t precision;   /* MPS_F32 / MPS_F64 / MPS_F32_N64                               */
+    int32_t reserved[7]; /* zero                                                          */
+} mps_params;
+
+/* Derived constants of a scene, as SetPara / AlcBkt compute them (kernel.cu:307-373). */
+typedef struct mps_info {
+    int32_t n_particles, n_fluid, n_wall;      /* nP, non-wall (FLD/GST), WLL/OBJ/OBJ2 */
+    int32_t nbx, nby, nbz, nbxyz;              /* bucket grid (kernel.cu:317-322)       */
+    double r, rp, db, dbinv;                   /* radii and bucket width (kernel.cu:309-315) */
+    double n0, lmd, n0_grad, lmd_grad;         /* lattice sums (kernel.cu:341-365)      */
+    int32_t numn0_grad, pad0;                  /* neighbour count of n0_grad            */
+    double rlim2, col, prs_coef, pmax, umax, dt, snd;
+    double minc[3], maxc[3];                   /* padded domain (kernel.cu:26-31)       */
+} mps_info;
+
+/* Device-side counters (host-side failure detection; nothing here traps the GPU). */
+typedef struct mps_counters {
+    int64_t steps;                 /* completed time steps                                  */
+    int32_t n_fluid_alive;         /* FLD particles                                         */
+    int32_t n_deleted;             /* GST particles among the non-wall particles            */
+    int32_t n_mirror_1;            /* mirrors alive after the first generation of the step  */
+    int32_t n_mirror_2;            /* mirrors alive after the second generation             */
+    int32_t err_mirror_slot;       /* corner mirror found no free slot (kernel.cu:868-874)  */
+    int32_t err_mirror_capacity;   /* mirror buffer full                                    */
+    int32_t err_cell_range;        /* a bucket index left the grid and was clamped          */
+    int32_t err_nan;               /* non-finite position met in a bucket build             */
+    int32_t reserved[6];
+} mps_counters;
+
+/* Per-particle diagnostic counters (mps_get_diag), column order of the int32 table. */
+enum {
+    MPS_DIAG_CELL = 0,      /* bucket index ib (kernel.cu:521-524), -1 for GST          */
+    MPS_DIAG_VSC_F = 1,     /* VscTrm fluid neighbours, dist <= r      (kernel.cu:1057) */
+    MPS_DIAG_VSC_M = 2,     /* VscTrm mirror neighbours                (kernel.cu:1092) */
+    MPS_DIAG_COL_F = 3,     /* ChkCol fluid, dist2 < rlim2             (kernel.cu:1211) */
+    MPS_DIAG_COL_W = 4,     /* ChkCol walls, dist2 < (0.45 l0)^2       (kernel.cu:1228) */
+    MPS_DIAG_COL_M = 5,     /* ChkCol mirrors                          (kernel.cu:1261) */
+    MPS_DIAG_PRS_F = 6,     /* MkPrs fluid, dist < rp                  (kernel.cu:1346) */
+    MPS_DIAG_PRS_M = 7,     /* MkPrs mirrors                           (kernel.cu:1376) */
+    MPS_DIAG_GRD_F = 8,     /* PrsGrdTrm fluid, dist2 < rp2            (kernel.cu:1730) */
+    MPS_DIAG_GRD_M = 9,     /* PrsGrdTrm mirrors (j != i)              (kernel.cu:1768) */
+    MPS_DIAG_GEN_W = 10,    /* GenMRR walls, dist2 <= r2               (kernel.cu:753)  */
+    MPS_DIAG_NCOL = 11
+};
+
+/* Steps of the reference's time loop, one per `class MPS` method (class.cuh:8-28). */
+enum {
+    MPS_PHASE_MKBKT = 0,          /* MPS::MkBkt          kernel.cu:532-550  */
+    MPS_PHASE_SURFACE_EDGE = 1,   /* MPS::Surface_Edge   kernel.cu:671-686  */
+    MPS_PHASE_RESETMRR = 2,       /* MPS::ResetMRR       kernel.cu:704-717  */
+    MPS_PHASE_GENMRR_NONSLIP = 3, /* MPS::GenMRR_nonslip kernel.cu:896-911  */
+    MPS_PHASE_MKBKT_MRR = 4,      /* MPS::MkBkt_MRR      kernel.cu:987-1010 */
+    MPS_PHASE_VSCTRM = 5,         /* MPS::VscTrm         kernel.cu:1122-1135 */
+    MPS_PHASE_UPPCL1 = 6,         /* MPS::UpPcl1         kernel.cu:1152-1165 */
+    MPS_PHASE_CHKCOL = 7,         /* MPS::ChkCol         kernel.cu:1289-1303 */
+    MPS_PHASE_MKPRS = 8,          /* MPS::MkPrs          kernel.cu:1414-1427 */
+    MPS_PHASE_PRSGRDTRM = 9,      /* MPS::PrsGrdTrm      kernel.cu:1798-1812 */
+    MPS_PHASE_UPPCL2 = 10,        /* MPS::UpPcl2         kernel.cu:1831-1844 */
+    MPS_PHASE_COUNT = 11
+};
+
+/* Handle options (mps_set_option). */
+enum {
+    MPS_OPT_DIAG = 0,        /* 1: record per-particle neighbour counts (slower)        */
+    MPS_OPT_GRAPH = 1,       /* 1: replay mps_step through a captured CUDA graph        */
+    MPS_OPT_BLOCK = 2,       /* threads per block of the neighbour passes (0 = tuned)   */
+    MPS_OPT_CELL_SKIP = 3    /* 1: skip bucket rows outside the radius (default 1)      */
+};
+
+typedef struct mps_handle mps_handle;
+
+/* ---- scene set-up ----------------------------------------------------------------- */
+
+/*
+ * Dam-break scene: a rectangular tank [0,L]^3 with single-layer walls on the faces
+ * selected by `wall_mask` (bit 0: x=0, 1: x=Lx, 2: y=0, 3: y=Ly, 4: z=0, 5: z=Lz), wall
+ * particles at in-plane positions ((p+1/2)l0, (q+1/2)l0) of each face, and a fluid block
+ * of nx*ny*nz particles at ((i+1/2)l0, (j+1/2)l0, (k+1/2)l0) + jitter.
+ * Replaces the scene the reference reads from initial.txt (kernel.cu:59-141).
+ */
+typedef struct mps_scene_desc {
+    double l0;                  /* spacing                                              */
+    double tank[3];             /* tank extent                                          */
+    int32_t block[3];           /* fluid particles along x, y, z                        */
+    int32_t wall_mask;          /* faces with walls (0x1f = open top)                   */
+    double jitter;              /* uniform jitter half-width as a fraction of l0        */
+    uint64_t seed;              /* mt19937_64 seed of the jitter                        */
+    double vel_sigma;           /* N(0, vel_sigma) initial velocity per component       */
+    uint64_t vel_seed;          /* mt19937_64 seed of the velocities                    */
+    double origin[3];           /* offset added to every position                       */
+} mps_scene_desc;
+
+/* Number of particles the scene will hold. */
+int mps_scene_dambreak_count(const mps_scene_desc* d, int32_t* n_out);
+/* Fill caller buffers (capacity >= count): typ[n], pos/vel/nrm as double SoA 3*n. */
+int mps_scene_dambreak(const mps_scene_desc* d, int32_t cap, int8_t* typ, double* pos,
+                       double* vel, double* nrm, int32_t* n_out);
+/* Fill `p` for a dam break: domain = tank, umax = sqrt(2|g|H), pmax = rho|g|H. */
+int mps_params_dambreak(const mps_scene_desc* d, double snd, double dt, double knm_vsc,
+                        double g_z, int32_t precision, mps_params* p);
+
+/* ---- handle life cycle ------------------------------------------------------------ */
+
+/*
+ * Create a solver for one scene. Replaces RdDat + AlcBkt + SetPara (kernel.cu:4-143,
+ * 307-478): derives the lattice constants, allocates device state, uploads the
+ * particles, builds the buckets and runs Surface_Edge (kernel.cu:1878-1879).
+ * Particles outside the padded domain become GST (RdDat drops them, kernel.cu:117).
+ */
+int mps_create(const mps_params* p, int32_t n, const int8_t* typ, const void* pos,
+               const void* vel, const void* nrm, mps_handle** out);
+
+/*
+ * Create one solver holding `nscenes` independent scenes that are advanced together.
+ * counts[s] particles of scene s are stored consecutively in the arrays; ids are
+ * global (scene s starts at sum(counts[0..s))). Every scene shares precision.
+ */
+int mps_create_batch(int32_t nscenes, const mps_params* p, const int32_t* counts,
+                     const int8_t* typ, const void* pos, const void* vel, const void* nrm,
+                     mps_handle** out);
+
+int mps_destroy(mps_handle* h);
+/* Queue the handle's work on `cuda_stream` (a cudaStream_t); NULL selects the handle's own
+ * non-blocking stream, which is the default. */
+int mps_set_stream(mps_handle* h, void* cuda_stream);
+int mps_set_option(mps_handle* h, int32_t option, int32_t value);
+int mps_synchronize(mps_handle* h);
+
+/* ---- time stepping ---------------------------------------------------------------- */
+
+/* Advance every scene by `nsteps` steps of the loop body kernel.cu:1904-1941. */
+int mps_step(mps_handle* h, int32_t nsteps);
+/* Run one method of the reference's step on its own (MPS_PHASE_*). */
+int mps_phase(mps_handle* h, int32_t phase);
+
+/* ---- state access (host buffers, id order; DevicetoHost, kernel.cu:1847-1869) ------- */
+
+int mps_get_info(mps_handle* h, int32_t scene, mps_info* out);
+/* Any pointer may be NULL. acc is the reference's d_Acc. */
+int mps_get_state(mps_handle* h, int8_t* typ, void* pos, void* vel, void* acc, void* prs,
+                  void* pav);
+/* Replace the non-wall state (walls are static and ignored here). typ in {FLD, GST}. */
+int mps_set_state(mps_handle* h, const int8_t* typ, const void* pos, const void* vel,
+                  const void* acc, const void* prs, const void* pav);
+/* WLLSE flags of every particle (Surface for non-walls), kernel.cu:553-668. */
+int mps_get_wall_flags(mps_handle* h, int8_t* wllse);
+/*
+ * Mirrors of the latest generation (`which` = 1: the set the viscosity / collision /
+ * density steps read, 2: the set the pressure gradient reads), sorted by slot id
+ * = i*MPS_NUM_MRR + k as in the reference's d_TypM layout (kernel.cu:689-893).
+ * pos is SoA with stride `cap`. *n_out receives the count even if it exceeds cap.
+ */
+int mps_get_mirrors(mps_handle* h, int32_t which, int32_t cap, int32_t* slot, void* pos,
+                    void* prs, int32_t* n_out);
+/* Per-particle diagnostic table [n_particles][MPS_DIAG_NCOL] and number density n_i. */
+int mps_get_diag(mps_handle* h, int32_t* table, void* ndens);
+int mps_get_counters(mps_handle* h, mps_counters* out);
+/*
+ * Integrals of scene `scene`: out[0..2] fluid centroid, out[3] kinetic energy per unit
+ * mass (sum |v|^2 / 2), out[4] surge front (max x of fluid), out[5] alive fluid count.
+ */
+int mps_get_integrals(mps_handle* h, int32_t scene, double out[6]);
+
+/* ---- errors ----------------------------------------------------------------------- */
+const char* mps_status_string(int32_t status);
+/* Text of the last failure on this thread (CUDA error string, argument check, ...). */
+const char* mps_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPS_B200_H */

@@ -1,0 +1,134 @@
+"""ctypes binding of ``libmps_b200.so`` (the C-ABI in ``include/mps_b200.h``).
+
+The library is loaded from this package directory. If it is missing or older than its
+sources it is rebuilt with nvcc; if that is impossible the import fails loudly -- there is no
+CPU fallback behind this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+from . import build as _build
+
+_lock = threading.Lock()
+_lib = None
+
+c_int8_p = C.POINTER(C.c_int8)
+c_int32_p = C.POINTER(C.c_int32)
+c_double_p = C.POINTER(C.c_double)
+
+# status codes / enums (mirror include/mps_b200.h)
+MPS_OK, MPS_ERR_ARG, MPS_ERR_CUDA, MPS_ERR_NOMEM, MPS_ERR_STATE = 0, 1, 2, 3, 4
+MPS_ERR_OVERFLOW, MPS_ERR_TIMEOUT, MPS_ERR_UNSUPPORTED, MPS_ERR_NODEVICE = 5, 6, 7, 8
+GST, FLD, WLL, OBJ, OBJ2, MRR = -1, 0, 1, 2, 3, 4
+SURFACE, EDGE = 0, 1
+NUM_MRR = 10
+F32, F64, F32_N64 = 0, 1, 2
+(PHASE_MKBKT, PHASE_SURFACE_EDGE, PHASE_RESETMRR, PHASE_GENMRR_NONSLIP, PHASE_MKBKT_MRR,
+ PHASE_VSCTRM, PHASE_UPPCL1, PHASE_CHKCOL, PHASE_MKPRS, PHASE_PRSGRDTRM, PHASE_UPPCL2) = range(11)
+OPT_DIAG, OPT_GRAPH, OPT_BLOCK, OPT_CELL_SKIP = 0, 1, 2, 3
+DIAG_COLUMNS = ["cell", "vsc_f", "vsc_m", "col_f", "col_w", "col_m", "prs_f", "prs_m",
+                "grd_f", "grd_m", "gen_w"]
+
+
+class mps_params(C.Structure):
+    _fields_ = [("pcl_dst", C.c_double), ("min", C.c_double * 3), ("max", C.c_double * 3),
+                ("g", C.c_double * 3), ("knm_vsc", C.c_double), ("col_rat", C.c_double),
+                ("dst_lmt_rat", C.c_double), ("rho", C.c_double), ("snd", C.c_double),
+                ("dt", C.c_double), ("umax", C.c_double), ("pmax", C.c_double),
+                ("precision", C.c_int32), ("reserved", C.c_int32 * 7)]
+
+
+class mps_info(C.Structure):
+    _fields_ = [("n_particles", C.c_int32), ("n_fluid", C.c_int32), ("n_wall", C.c_int32),
+                ("nbx", C.c_int32), ("nby", C.c_int32), ("nbz", C.c_int32), ("nbxyz", C.c_int32),
+                ("r", C.c_double), ("rp", C.c_double), ("db", C.c_double), ("dbinv", C.c_double),
+                ("n0", C.c_double), ("lmd", C.c_double), ("n0_grad", C.c_double),
+                ("lmd_grad", C.c_double), ("numn0_grad", C.c_int32), ("pad0", C.c_int32),
+                ("rlim2", C.c_double), ("col", C.c_double), ("prs_coef", C.c_double),
+                ("pmax", C.c_double), ("umax", C.c_double), ("dt", C.c_double),
+                ("snd", C.c_double), ("minc", C.c_double * 3), ("maxc", C.c_double * 3)]
+
+
+class mps_counters(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("n_fluid_alive", C.c_int32), ("n_deleted", C.c_int32),
+                ("n_mirror_1", C.c_int32), ("n_mirror_2", C.c_int32),
+                ("err_mirror_slot", C.c_int32), ("err_mirror_capacity", C.c_int32),
+                ("err_cell_range", C.c_int32), ("err_nan", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
+
+
+class mps_scene_desc(C.Structure):
+    _fields_ = [("l0", C.c_double), ("tank", C.c_double * 3), ("block", C.c_int32 * 3),
+                ("wall_mask", C.c_int32), ("jitter", C.c_double), ("seed", C.c_uint64),
+                ("vel_sigma", C.c_double), ("vel_seed", C.c_uint64), ("origin", C.c_double * 3)]
+
+
+# symbol -> (restype, argtypes); every symbol include/mps_b200.h declares
+SIGNATURES = {
+    "mps_scene_dambreak_count": (C.c_int, [C.POINTER(mps_scene_desc), c_int32_p]),
+    "mps_scene_dambreak": (C.c_int, [C.POINTER(mps_scene_desc), C.c_int32, c_int8_p, c_double_p,
+                                     c_double_p, c_double_p, c_int32_p]),
+    "mps_params_dambreak": (C.c_int, [C.POINTER(mps_scene_desc), C.c_double, C.c_double,
+                                      C.c_double, C.c_double, C.c_int32, C.POINTER(mps_params)]),
+    "mps_create": (C.c_int, [C.POINTER(mps_params), C.c_int32, c_int8_p, C.c_void_p, C.c_void_p,
+                             C.c_void_p, C.POINTER(C.c_void_p)]),
+    "mps_create_batch": (C.c_int, [C.c_int32, C.POINTER(mps_params), c_int32_p, c_int8_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "mps_destroy": (C.c_int, [C.c_void_p]),
+    "mps_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mps_set_option": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    "mps_synchronize": (C.c_int, [C.c_void_p]),
+    "mps_step": (C.c_int, [C.c_void_p, C.c_int32]),
+    "mps_phase": (C.c_int, [C.c_void_p, C.c_int32]),
+    "mps_get_info": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(mps_info)]),
+    "mps_get_state": (C.c_int, [C.c_void_p, c_int8_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.c_void_p]),
+    "mps_set_state": (C.c_int, [C.c_void_p, c_int8_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_void_p, C.c_void_p]),
+    "mps_get_wall_flags": (C.c_int, [C.c_void_p, c_int8_p]),
+    "mps_get_mirrors": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, c_int32_p, C.c_void_p,
+                                  C.c_void_p, c_int32_p]),
+    "mps_get_diag": (C.c_int, [C.c_void_p, c_int32_p, C.c_void_p]),
+    "mps_get_counters": (C.c_int, [C.c_void_p, C.POINTER(mps_counters)]),
+    "mps_get_integrals": (C.c_int, [C.c_void_p, C.c_int32, c_double_p]),
+    "mps_status_string": (C.c_char_p, [C.c_int32]),
+    "mps_last_error": (C.c_char_p, []),
+}
+
+
+class MPSError(RuntimeError):
+    def __init__(self, code: int, where: str, detail: str):
+        super().__init__(f"{where}: status {code} ({detail})")
+        self.code = code
+
+
+def lib():
+    """Load (building if needed) the native library."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = _build.LIB
+        if not _build.up_to_date(path):
+            _build.build()
+        L = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+        return _lib
+
+
+def check(rc: int, where: str) -> None:
+    if rc != MPS_OK:
+        L = lib()
+        msg = (L.mps_last_error() or b"").decode(errors="replace")
+        raise MPSError(rc, where, msg or L.mps_status_string(rc).decode())
+
+
+def library_path() -> str:
+    return os.path.abspath(_build.LIB)

@@ -1,0 +1,218 @@
+// mps_api.cu -- the C-ABI of include/mps_b200.h over the templated solver.
+//
+// One handle owns the device state of one or more scenes. The reference keeps that state
+// in public members of `class MPS` (class.cuh:49-141) and drives it from ClcMPS
+// (kernel.cu:1872-1943) with a blocking cudaDeviceSynchronize after every kernel; here the
+// whole step is queued on one stream (optionally replayed as a CUDA graph) and nothing
+// synchronises until the caller reads data back.
+#include "mps_solver.cuh"
+
+namespace mps {
+thread_local std::string g_last_error;
+}  // namespace mps
+
+// =========================================================================================
+// C-ABI
+// =========================================================================================
+using mps::ApiError;
+using mps::SolverBase;
+
+struct mps_handle {
+    std::unique_ptr<SolverBase> s;
+};
+
+namespace {
+int fail(int code, const std::string& msg) {
+    mps::g_last_error = msg;
+    return code;
+}
+
+template <class F> int guarded(mps_handle* h, F&& f) {
+    if (!h || !h->s) return fail(MPS_ERR_ARG, "null handle");
+    try {
+        cudaError_t e = cudaSetDevice(h->s->dev);
+        if (e != cudaSuccess) return fail(MPS_ERR_CUDA, cudaGetErrorString(e));
+        f(*h->s);
+        return MPS_OK;
+    } catch (const ApiError& e) {
+        return fail(e.code, e.what());
+    } catch (const std::exception& e) {
+        return fail(MPS_ERR_CUDA, e.what());
+    }
+}
+
+int check_params(const mps_params& p) {
+    if (!(p.pcl_dst > 0) || !(p.dt > 0) || !(p.rho > 0) || !(p.snd >= 0))
+        return fail(MPS_ERR_ARG, "pcl_dst, dt and rho must be positive, snd non-negative");
+    for (int d = 0; d < 3; ++d)
+        if (!(p.max[d] > p.min[d])) return fail(MPS_ERR_ARG, "domain max must exceed min");
+    if (p.precision < 0 || p.precision > 2) return fail(MPS_ERR_ARG, "unknown precision");
+    return MPS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int mps_create_batch(int32_t nscenes, const mps_params* p, const int32_t* counts,
+                     const int8_t* typ, const void* pos, const void* vel, const void* nrm,
+                     mps_handle** out) {
+    if (!out) return fail(MPS_ERR_ARG, "out is null");
+    *out = nullptr;
+    if (nscenes <= 0 || !p || !counts || !typ || !pos || !vel || !nrm)
+        return fail(MPS_ERR_ARG, "null argument or no scenes");
+    long long total = 0;
+    for (int s = 0; s < nscenes; ++s) {
+        int rc = check_params(p[s]);
+        if (rc) return rc;
+        if (p[s].precision != p[0].precision)
+            return fail(MPS_ERR_ARG, "every scene of a batch must use the same precision");
+        if (counts[s] < 0) return fail(MPS_ERR_ARG, "negative particle count");
+        total += counts[s];
+    }
+    if (total * mps::kNumMRR > 2000000000LL) return fail(MPS_ERR_ARG, "too many particles");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(MPS_ERR_NODEVICE, "no CUDA device");
+    }
+    auto* h = new mps_handle();
+    try {
+        if (p[0].precision == 1)
+            h->s.reset(mps::make_solver_f64(nscenes, p, counts, typ, pos, vel, nrm));
+        else if (p[0].precision == 2)
+            h->s.reset(mps::make_solver_mix(nscenes, p, counts, typ, pos, vel, nrm));
+        else
+            h->s.reset(mps::make_solver_f32(nscenes, p, counts, typ, pos, vel, nrm));
+    } catch (const ApiError& e) {
+        delete h;
+        return fail(e.code, e.what());
+    } catch (const std::exception& e) {
+        delete h;
+        return fail(MPS_ERR_CUDA, e.what());
+    }
+    *out = h;
+    return MPS_OK;
+}
+
+int mps_create(const mps_params* p, int32_t n, const int8_t* typ, const void* pos,
+               const void* vel, const void* nrm, mps_handle** out) {
+    return mps_create_batch(1, p, &n, typ, pos, vel, nrm, out);
+}
+
+int mps_destroy(mps_handle* h) {
+    if (!h) return MPS_OK;
+    if (h->s) {
+        cudaSetDevice(h->s->dev);
+        cudaStreamSynchronize(h->s->stream);
+    }
+    delete h;
+    return MPS_OK;
+}
+
+int mps_set_stream(mps_handle* h, void* stream) {
+    return guarded(h, [&](SolverBase& s) {
+        CK(cudaStreamSynchronize(s.stream));
+        // NULL selects the handle's own stream again
+        s.stream = stream ? static_cast<cudaStream_t>(stream) : s.own_stream;
+        s.invalidate_graph();
+    });
+}
+
+int mps_set_option(mps_handle* h, int32_t opt, int32_t value) {
+    return guarded(h, [&](SolverBase& s) {
+        switch (opt) {
+            case MPS_OPT_DIAG: s.diag_on = value != 0; break;
+            case MPS_OPT_GRAPH: s.graph_on = value != 0; s.invalidate_graph(); break;
+            case MPS_OPT_BLOCK:
+                if (value != 0 && (value < 32 || value > 128 || value % 32))
+                    throw ApiError(MPS_ERR_ARG, "block must be 0 or a multiple of 32 in [32, 128]");
+                s.block = value ? value : 128;
+                s.invalidate_graph();
+                break;
+            case MPS_OPT_CELL_SKIP: s.skip_opt = value != 0; s.invalidate_graph(); break;
+            default: throw ApiError(MPS_ERR_ARG, "unknown option");
+        }
+    });
+}
+
+int mps_synchronize(mps_handle* h) {
+    return guarded(h, [&](SolverBase& s) { CK(cudaStreamSynchronize(s.stream)); });
+}
+
+int mps_step(mps_handle* h, int32_t nsteps) {
+    if (nsteps < 0) return fail(MPS_ERR_ARG, "negative step count");
+    return guarded(h, [&](SolverBase& s) { s.step(nsteps); });
+}
+
+int mps_phase(mps_handle* h, int32_t phase) {
+    return guarded(h, [&](SolverBase& s) { s.phase(phase); });
+}
+
+int mps_get_info(mps_handle* h, int32_t scene, mps_info* out) {
+    return guarded(h, [&](SolverBase& s) {
+        if (!out || scene < 0 || scene >= s.nscene) throw ApiError(MPS_ERR_ARG, "bad scene");
+        *out = s.infos[scene];
+        out->n_particles = s.counts[scene];
+        out->n_fluid = s.nF;
+        out->n_wall = s.nW;
+    });
+}
+
+int mps_get_state(mps_handle* h, int8_t* typ, void* pos, void* vel, void* acc, void* prs,
+                  void* pav) {
+    return guarded(h, [&](SolverBase& s) { s.get_state(typ, pos, vel, acc, prs, pav); });
+}
+
+int mps_set_state(mps_handle* h, const int8_t* typ, const void* pos, const void* vel,
+                  const void* acc, const void* prs, const void* pav) {
+    return guarded(h, [&](SolverBase& s) { s.set_state(typ, pos, vel, acc, prs, pav); });
+}
+
+int mps_get_wall_flags(mps_handle* h, int8_t* wllse) {
+    if (!wllse) return fail(MPS_ERR_ARG, "null buffer");
+    return guarded(h, [&](SolverBase& s) { s.get_wall_flags(wllse); });
+}
+
+int mps_get_mirrors(mps_handle* h, int32_t which, int32_t cap, int32_t* slot, void* pos,
+                    void* prs, int32_t* n_out) {
+    if (which < 0 || which > 2 || cap < 0) return fail(MPS_ERR_ARG, "bad mirror request");
+    return guarded(h, [&](SolverBase& s) {
+        int n = s.get_mirrors(which, cap, slot, pos, prs);
+        if (n_out) *n_out = n;
+    });
+}
+
+int mps_get_diag(mps_handle* h, int32_t* table, void* ndens) {
+    return guarded(h, [&](SolverBase& s) { s.get_diag(table, ndens); });
+}
+
+int mps_get_counters(mps_handle* h, mps_counters* out) {
+    if (!out) return fail(MPS_ERR_ARG, "null buffer");
+    return guarded(h, [&](SolverBase& s) { s.get_counters(out); });
+}
+
+int mps_get_integrals(mps_handle* h, int32_t scene, double out[6]) {
+    return guarded(h, [&](SolverBase& s) {
+        if (!out || scene < 0 || scene >= s.nscene) throw ApiError(MPS_ERR_ARG, "bad scene");
+        s.integrals(scene, out);
+    });
+}
+
+const char* mps_status_string(int32_t st) {
+    switch (st) {
+        case MPS_OK: return "ok";
+        case MPS_ERR_ARG: return "invalid argument";
+        case MPS_ERR_CUDA: return "CUDA error";
+        case MPS_ERR_NOMEM: return "out of memory";
+        case MPS_ERR_STATE: return "invalid state";
+        case MPS_ERR_OVERFLOW: return "capacity exceeded";
+        case MPS_ERR_TIMEOUT: return "device wait timed out";
+        case MPS_ERR_UNSUPPORTED: return "unsupported";
+        case MPS_ERR_NODEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char* mps_last_error(void) { return mps::g_last_error.c_str(); }
+
+}  // extern "C"

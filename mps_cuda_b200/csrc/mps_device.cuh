@@ -1,0 +1,474 @@
+// mps_device.cuh -- per-particle physics of the explicit MPS step, as device functions.
+//
+// Every function here is shared by the fused step kernels and by the one-method-per-launch
+// kernels behind mps_phase(), so both paths round identically. Arithmetic follows one
+// fixed form (the build uses -fmad=false; each fused multiply-add is an explicit
+// __fma_rn), neighbour buckets are visited z, y, x ascending and particles inside a bucket
+// in ascending id, so a result depends only on its inputs.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "mps_types.h"
+
+namespace mps {
+
+__device__ __forceinline__ float fmaR(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmaR(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float sqrtR(float a) { return sqrtf(a); }
+__device__ __forceinline__ double sqrtR(double a) { return sqrt(a); }
+
+template <class R> __device__ __forceinline__ R dot3(R ax, R ay, R az, R bx, R by, R bz) {
+    return fmaR(az, bz, fmaR(ay, by, ax * bx));
+}
+// WEI_grad(dst, re), const.cuh:46
+template <class R> __device__ __forceinline__ R wei_grad(R d, R re) { return (re / d) - (d / re); }
+
+template <class R> __device__ __forceinline__ V4<R> ldv(const V4<R>* p) {
+    return __ldg(reinterpret_cast<const V4<R>*>(p));
+}
+__device__ __forceinline__ V4<float> ldg4(const V4<float>* p) {
+    float4 v = __ldg(reinterpret_cast<const float4*>(p));
+    return V4<float>{v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ V4<double> ldg4(const V4<double>* p) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    double2 a = __ldg(q), b = __ldg(q + 1);
+    return V4<double>{a.x, a.y, b.x, b.y};
+}
+
+// scene of a global particle id (scenes are stored in ascending pbase)
+template <class R, class RN>
+__device__ __forceinline__ int scene_of(const SceneDev<R, RN>* sc, int nscene, int pid) {
+    int lo = 0, hi = nscene - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&sc[mid].pbase) <= pid) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Bucket coordinates, kernel.cu:521-524. Returns false if the index left the grid (then
+// it is clamped to the interior so that the 27-bucket walk stays inside the grid).
+template <class R, class RN>
+__device__ __forceinline__ bool cell_of(const SceneDev<R, RN>& sc, R x, R y, R z, int& ix,
+                                        int& iy, int& iz) {
+    ix = int((x - sc.minc[0]) * sc.dbinv) + 1;
+    iy = int((y - sc.minc[1]) * sc.dbinv) + 1;
+    iz = int((z - sc.minc[2]) * sc.dbinv) + 1;
+    bool ok = ix >= 1 && ix <= sc.nbx - 2 && iy >= 1 && iy <= sc.nby - 2 && iz >= 1 &&
+              iz <= sc.nbz - 2;
+    if (!ok) {
+        ix = min(max(ix, 1), sc.nbx - 2);
+        iy = min(max(iy, 1), sc.nby - 2);
+        iz = min(max(iz, 1), sc.nbz - 2);
+    }
+    return ok;
+}
+
+// Position of a particle inside its bucket, used to skip bucket rows that cannot hold a
+// neighbour inside the radius. Skipping never reorders the neighbours that remain.
+template <class R> struct RowCtx {
+    int ix, iy, iz;
+    R dxl, dxh, dyl, dyh, dzl, dzh;
+};
+
+template <class R, class RN>
+__device__ __forceinline__ RowCtx<R> row_ctx(const SceneDev<R, RN>& sc, R x, R y, R z, int ix,
+                                             int iy, int iz) {
+    RowCtx<R> c;
+    c.ix = ix; c.iy = iy; c.iz = iz;
+    R xl = sc.minc[0] + R(ix - 1) * sc.db;
+    R yl = sc.minc[1] + R(iy - 1) * sc.db;
+    R zl = sc.minc[2] + R(iz - 1) * sc.db;
+    c.dxl = x - xl; c.dxh = (xl + sc.db) - x;
+    c.dyl = y - yl; c.dyh = (yl + sc.db) - y;
+    c.dzl = z - zl; c.dzh = (zl + sc.db) - z;
+    return c;
+}
+
+// Visit the 27 buckets around c (z, y, x ascending); a row of three x-adjacent buckets is
+// one contiguous range of the sorted arrays. `B` is (radius + margin)^2: a row or an end
+// bucket whose nearest point lies farther than that is not visited.
+template <class R, class RN, class F>
+__device__ __forceinline__ void for_rows(const SceneDev<R, RN>& sc, const int* __restrict__ cs,
+                                         const RowCtx<R>& c, R B, F&& f) {
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz) {
+        R ddz = dz < 0 ? c.dzl : (dz > 0 ? c.dzh : R(0));
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+            R ddy = dy < 0 ? c.dyl : (dy > 0 ? c.dyh : R(0));
+            R dyz2 = ddy * ddy + ddz * ddz;
+            if (dyz2 > B) continue;
+            int jl = (dyz2 + c.dxl * c.dxl <= B) ? c.ix - 1 : c.ix;
+            int jh = (dyz2 + c.dxh * c.dxh <= B) ? c.ix + 1 : c.ix;
+            int row = sc.cbase + (c.iz + dz) * sc.nbxy + (c.iy + dy) * sc.nbx;
+            int lo = __ldg(cs + row + jl), hi = __ldg(cs + row + jh + 1);
+            for (int j = lo; j < hi; ++j) f(j);
+        }
+    }
+}
+
+// ---- views ------------------------------------------------------------------------------
+template <class R> struct WallView {
+    const int* cs;
+    const V4<R>* pos;
+    const V4<R>* nrm;
+    const V4<R>* vel;
+    const int8_t* wse;
+    const int8_t* typ;
+};
+template <class R> struct MirrorView {
+    const int* cs;
+    const V4<R>* pos;  // w = PrsM
+    const int* slot;
+};
+template <class R> struct MirrorSink {
+    V4<R>* pos;
+    int* slot;
+    int cap;
+};
+
+// ---- VscTrm sum (kernel.cu:1037-1107) ----------------------------------------------------
+// mirror part: VelM = 0 (kernel.cu:834-836)
+template <class R, class RN>
+__device__ __forceinline__ void visc_sum_mirrors(const SceneDev<R, RN>& sc, const RowCtx<R>& c, R x,
+                                                 R y, R z, R ux, R uy, R uz,
+                                                 const MirrorView<R>& m, R B, R& sx, R& sy, R& sz,
+                                                 int& cm) {
+    for_rows(sc, m.cs, c, B, [&](int k) {
+        V4<R> q = ldg4(m.pos + k);
+        R dx = q.x - x, dy = q.y - y, dz = q.z - z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (d2 <= sc.r_le) {
+            R d = sqrtR(d2);
+            R w = sc.two_l0 / (d2 * d);
+            sx = fmaR(R(0) - ux, w, sx);
+            sy = fmaR(R(0) - uy, w, sy);
+            sz = fmaR(R(0) - uz, w, sz);
+            ++cm;
+        }
+    });
+}
+
+template <class R, class RN>
+__device__ __forceinline__ void visc_sum(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
+                                         R x, R y, R z, R ux, R uy, R uz,
+                                         const int* __restrict__ cs,
+                                         const V4<R>* __restrict__ pos,
+                                         const V4<R>* __restrict__ vel, const MirrorView<R>& m,
+                                         R B, R& sx, R& sy, R& sz, int& cf, int& cm) {
+    for_rows(sc, cs, c, B, [&](int j) {
+        if (j == s) return;
+        V4<R> q = ldg4(pos + j);
+        R dx = q.x - x, dy = q.y - y, dz = q.z - z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (d2 <= sc.r_le) {  // dist <= r
+            V4<R> u = ldg4(vel + j);
+            R d = sqrtR(d2);
+            R w = sc.two_l0 / (d2 * d);
+            sx = fmaR(u.x - ux, w, sx);
+            sy = fmaR(u.y - uy, w, sy);
+            sz = fmaR(u.z - uz, w, sz);
+            ++cf;
+        }
+    });
+    visc_sum_mirrors(sc, c, x, y, z, ux, uy, uz, m, B, sx, sy, sz, cm);
+}
+
+// ---- ChkPcl (kernel.cu:481-513); returns false when the particle is deleted --------------
+template <class R, class RN>
+__device__ __forceinline__ bool chkpcl(const SceneDev<R, RN>& sc, R x, R y, R z, R& ux, R& uy,
+                                       R& uz) {
+    if (x < sc.hi[0] && x > sc.lo[0] && y < sc.hi[1] && y > sc.lo[1] && z < sc.hi[2] &&
+        z > sc.lo[2]) {
+        R u = sqrtR(dot3(ux, uy, uz, ux, uy, uz));
+        if (u > sc.umax) {
+            R f = sc.umax / u;
+            ux *= f; uy *= f; uz *= f;
+        }
+        return true;
+    }
+    return false;
+}
+
+// ---- ChkCol (kernel.cu:1193-1275) and MkPrs (kernel.cu:1328-1386) sums ------------------
+template <class R>
+__device__ __forceinline__ void col_hit(R colfac, R ux, R uy, R uz, R jx, R jy, R jz, R dx, R dy,
+                                        R dz, R d2, R& wx, R& wy, R& wz) {
+    R f = dot3(ux - jx, uy - jy, uz - jz, dx, dy, dz);
+    if (f > R(0)) {
+        f = f * (colfac / d2);
+        wx = fmaR(-dx, f, wx);
+        wy = fmaR(-dy, f, wy);
+        wz = fmaR(-dz, f, wz);
+    }
+}
+
+template <class R, class RN>
+__device__ __forceinline__ void dens_add(const SceneDev<R, RN>& sc, R d2, RN& ni) {
+    if (sizeof(RN) == sizeof(R)) {
+        R d = sqrtR(d2);
+        ni += RN(wei_grad(d, sc.rp));
+    } else {
+        RN d = sqrtR(RN(d2));
+        ni += wei_grad(d, sc.rp_n);
+    }
+}
+
+// wall (collision only) and mirror parts, visited after the fluid neighbours
+template <class R, class RN, bool COL, bool DENS>
+__device__ __forceinline__ void col_dens_walls_mirrors(const SceneDev<R, RN>& sc, const RowCtx<R>& c,
+                                                       R x, R y, R z, R ux, R uy, R uz,
+                                                       const WallView<R>& wl,
+                                                       const MirrorView<R>& m, bool skip, R& wx,
+                                                       R& wy, R& wz, RN& ni, int* cnt) {
+    const R inf = R(INFINITY);
+    const R Bf = !skip ? inf : (COL && DENS ? sc.skip_rc : (DENS ? sc.skip_rp : sc.skip_rl));
+    if (COL) {
+        for_rows(sc, wl.cs, c, skip ? sc.skip_rw : inf, [&](int j) {
+            V4<R> q = ldg4(wl.pos + j);
+            R dx = q.x - x, dy = q.y - y, dz = q.z - z;
+            R d2 = dot3(dx, dy, dz, dx, dy, dz);
+            if (d2 < sc.rlimw2) {
+                V4<R> u = ldg4(wl.vel + j);
+                col_hit(sc.colfac, ux, uy, uz, u.x, u.y, u.z, dx, dy, dz, d2, wx, wy, wz);
+                ++cnt[1];
+            }
+        });
+    }
+    for_rows(sc, m.cs, c, Bf, [&](int k) {
+        V4<R> q = ldg4(m.pos + k);
+        R dx = q.x - x, dy = q.y - y, dz = q.z - z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (COL && d2 < sc.rlim2) {
+            col_hit(sc.colfac, ux, uy, uz, R(0), R(0), R(0), dx, dy, dz, d2, wx, wy, wz);
+            ++cnt[2];
+        }
+        if (DENS && d2 <= sc.rp_lt) {
+            dens_add(sc, d2, ni);
+            ++cnt[4];
+        }
+    });
+}
+
+template <class R, class RN, bool COL, bool DENS>
+__device__ __forceinline__ void col_dens_sum(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
+                                             R x, R y, R z, R ux, R uy, R uz,
+                                             const int* __restrict__ cs,
+                                             const V4<R>* __restrict__ pos,
+                                             const V4<R>* __restrict__ vel,
+                                             const WallView<R>& wl, const MirrorView<R>& m,
+                                             bool skip, R& wx, R& wy, R& wz, RN& ni, int* cnt) {
+    const R inf = R(INFINITY);
+    const R Bf = !skip ? inf : (COL && DENS ? sc.skip_rc : (DENS ? sc.skip_rp : sc.skip_rl));
+    for_rows(sc, cs, c, Bf, [&](int j) {
+        if (j == s) return;
+        V4<R> q = ldg4(pos + j);
+        R dx = q.x - x, dy = q.y - y, dz = q.z - z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (COL && d2 < sc.rlim2) {
+            V4<R> u = ldg4(vel + j);
+            col_hit(sc.colfac, ux, uy, uz, u.x, u.y, u.z, dx, dy, dz, d2, wx, wy, wz);
+            ++cnt[0];
+        }
+        if (DENS && d2 <= sc.rp_lt) {  // dist < rp
+            dens_add(sc, d2, ni);
+            ++cnt[3];
+        }
+    });
+    col_dens_walls_mirrors<R, RN, COL, DENS>(sc, c, x, y, z, ux, uy, uz, wl, m, skip, wx, wy, wz,
+                                             ni, cnt);
+}
+
+// explicit equation of state with clamps, kernel.cu:1388-1406
+template <class R, class RN>
+__device__ __forceinline__ R eos(const SceneDev<R, RN>& sc, RN ni) {
+    RN p = RN(ni > sc.n0g ? 1 : 0) * (ni - sc.n0g) * sc.prs_coef * sc.rho;
+    if (p <= sc.pmax && p >= RN(0)) {
+    } else {
+        p = (p > sc.pmax) ? sc.pmax : RN(0);
+    }
+    return R(p);
+}
+
+// ---- PrsGrdTrm (kernel.cu:1678-1791) ----------------------------------------------------
+// mirror part; the reference skips the mirror whose slot index equals i (kernel.cu:1759).
+// Slots are stored as global_owner_id * NumMRR + k: the local slot is that minus
+// NumMRR * pbase, the local particle index is pid_local.
+template <class R, class RN>
+__device__ __forceinline__ void grad_sum_mirrors(const SceneDev<R, RN>& sc, const RowCtx<R>& c,
+                                                 int pid_local, R x, R y, R z, R pmin,
+                                                 const MirrorView<R>& m, bool skip, R& sx, R& sy,
+                                                 R& sz, int& cm) {
+    const R B = skip ? sc.skip_rp : R(INFINITY);
+    const int skip_slot = pid_local + kNumMRR * sc.pbase;
+    for_rows(sc, m.cs, c, B, [&](int k) {
+        if (__ldg(m.slot + k) == skip_slot) return;
+        V4<R> q = ldg4(m.pos + k);
+        R dx = q.x - x, dy = q.y - y, dz = q.z - z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (d2 < sc.rp2) {
+            R d = sqrtR(d2);
+            R w = wei_grad(d, sc.rp) / d2;
+            R pw = (q.w - pmin) * w;
+            sx = fmaR(pw, dx, sx);
+            sy = fmaR(pw, dy, sy);
+            sz = fmaR(pw, dz, sz);
+            ++cm;
+        }
+    });
+}
+
+template <class R, class RN>
+__device__ __forceinline__ void grad_sum(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
+                                         int pid_local, R x, R y, R z, R pi,
+                                         const int* __restrict__ cs,
+                                         const V4<R>* __restrict__ pos,
+                                         const R* __restrict__ prs, const MirrorView<R>& m,
+                                         bool skip, R& sx, R& sy, R& sz, int& cf, int& cm) {
+    R B = skip ? sc.skip_rp : R(INFINITY);
+    R pmin = pi;
+    for_rows(sc, cs, c, B, [&](int j) {
+        if (j == s) return;
+        V4<R> q = ldg4(pos + j);
+        R dx = q.x - x, dy = q.y - y, dz = q.z - z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (d2 < sc.rp2) {
+            R pj = __ldg(prs + j);
+            if (pj < pmin) pmin = pj;
+        }
+    });
+    for_rows(sc, cs, c, B, [&](int j) {
+        if (j == s) return;
+        V4<R> q = ldg4(pos + j);
+        R dx = q.x - x, dy = q.y - y, dz = q.z - z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (d2 < sc.rp2) {
+            R d = sqrtR(d2);
+            R w = wei_grad(d, sc.rp) / d2;
+            R pw = (__ldg(prs + j) - pmin) * w;
+            sx = fmaR(pw, dx, sx);
+            sy = fmaR(pw, dy, sy);
+            sz = fmaR(pw, dz, sz);
+            ++cf;
+        }
+    });
+    grad_sum_mirrors(sc, c, pid_local, x, y, z, pmin, m, skip, sx, sy, sz, cm);
+}
+
+// ---- MRRinout cull of one mirror (kernel.cu:932-985); true = keep -----------------------
+template <class R, class RN>
+__device__ __forceinline__ bool cull_keep(const SceneDev<R, RN>& sc, R mx, R my, R mz,
+                                          const WallView<R>& wl, bool skip, int* err_cell) {
+    int ix, iy, iz;
+    if (!cell_of(sc, mx, my, mz, ix, iy, iz)) atomicAdd(err_cell, 1);
+    RowCtx<R> c = row_ctx(sc, mx, my, mz, ix, iy, iz);
+    bool found = false;
+    R wd = sc.wall_dist0;
+    R wx = 0, wy = 0, wz = 0, nx = 0, ny = 0, nz = 0;
+    for_rows(sc, wl.cs, c, skip ? sc.skip_r : R(INFINITY), [&](int j) {
+        V4<R> q = ldg4(wl.pos + j);
+        R dx = mx - q.x, dy = my - q.y, dz = mz - q.z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (d2 <= sc.r_le) {  // dist <= r
+            R d = sqrtR(d2);
+            if (d < wd) {
+                found = true;
+                wd = d;
+                V4<R> nv = ldg4(wl.nrm + j);
+                nx = nv.x; ny = nv.y; nz = nv.z;
+                wx = q.x; wy = q.y; wz = q.z;
+            }
+        }
+    });
+    R inout = dot3(mx - wx, my - wy, mz - wz, nx, ny, nz);
+    return !(found && inout >= R(0));
+}
+
+// ---- GenMRR_nonslip for one fluid particle (kernel.cu:726-891) ---------------------------
+// Appends the mirrors (culled on the spot when CULL) to `out`; returns the number of walls
+// inside r (diagnostic).
+template <class R, class RN, bool CULL>
+__device__ __forceinline__ int gen_mirrors(const SceneDev<R, RN>& sc, const RowCtx<R>& c, R x,
+                                           R y, R z, R P, int slot_base, const WallView<R>& wl,
+                                           bool skip, const MirrorSink<R>& out,
+                                           DevCounters* cnt) {
+    int reg[kNumMRR], edg[kNumMRR];
+    R rn[kNumMRR][3], en[kNumMRR][3];
+    int nreg = 0, nedge = 0, nwall = 0;
+    for_rows(sc, wl.cs, c, skip ? sc.skip_r : R(INFINITY), [&](int j) {
+        V4<R> q = ldg4(wl.pos + j);
+        R dx = x - q.x, dy = y - q.y, dz = z - q.z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (!(d2 <= sc.r2)) return;
+        ++nwall;
+        V4<R> nv = ldg4(wl.nrm + j);
+        bool dup = false;
+        for (int k = 0; k < nreg; ++k)
+            if (rn[k][0] == nv.x && rn[k][1] == nv.y && rn[k][2] == nv.z) dup = true;
+        if (!dup && nreg < kNumMRR) {
+            reg[nreg] = j;
+            rn[nreg][0] = nv.x; rn[nreg][1] = nv.y; rn[nreg][2] = nv.z;
+            ++nreg;
+        }
+        if (__ldg(wl.wse + j) == kEDGE) {
+            bool edup = false;
+            for (int k = 0; k < nedge; ++k)
+                if (en[k][0] == nv.x && en[k][1] == nv.y && en[k][2] == nv.z) edup = true;
+            if (!edup && nedge < kNumMRR) {
+                edg[nedge] = j;
+                en[nedge][0] = nv.x; en[nedge][1] = nv.y; en[nedge][2] = nv.z;
+                ++nedge;
+            }
+        }
+    });
+    if (nreg == 0) return nwall;
+    auto emit = [&](R mx, R my, R mz, int slot) {
+        if (CULL && !cull_keep(sc, mx, my, mz, wl, skip, &cnt->err_cell)) return;
+        int idx = atomicAdd(&cnt->mirror_raw, 1);
+        if (idx < out.cap) {
+            out.pos[idx] = V4<R>{mx, my, mz, P};
+            out.slot[idx] = slot;
+        } else {
+            atomicAdd(&cnt->err_capacity, 1);
+        }
+    };
+    // face mirrors (kernel.cu:811-838)
+    for (int k = 0; k < nreg; ++k) {
+        V4<R> q = ldg4(wl.pos + reg[k]);
+        R pwx = x - q.x, pwy = y - q.y, pwz = z - q.z;
+        R pw = dot3(pwx, pwy, pwz, rn[k][0], rn[k][1], rn[k][2]);
+        if (pw < R(0)) continue;
+        R dist = pw / sqrtR(dot3(rn[k][0], rn[k][1], rn[k][2], rn[k][0], rn[k][1], rn[k][2]));
+        R t2 = R(2) * dist;
+        emit(fmaR(-t2, rn[k][0], q.x + pwx), fmaR(-t2, rn[k][1], q.y + pwy),
+             fmaR(-t2, rn[k][2], q.z + pwz), slot_base + k);
+    }
+    // corner mirror through the last edge wall (kernel.cu:841-887)
+    if (nedge >= 2) {
+        R sx = 0, sy = 0, sz = 0;
+        for (int k = 0; k < nedge; ++k) {
+            sx += en[k][0]; sy += en[k][1]; sz += en[k][2];
+        }
+        V4<R> q = ldg4(wl.pos + edg[nedge - 1]);
+        R pwx = x - q.x, pwy = y - q.y, pwz = z - q.z;
+        R as = sqrtR(dot3(sx, sy, sz, sx, sy, sz));
+        sx /= as; sy /= as; sz /= as;
+        R pw = dot3(pwx, pwy, pwz, sx, sy, sz);
+        if (pw >= R(0)) {
+            R dist = pw / sqrtR(dot3(sx, sy, sz, sx, sy, sz));
+            if (nreg >= kNumMRR) {
+                atomicAdd(&cnt->err_mirror_slot, 1);
+            } else {
+                R t2 = R(2) * dist;
+                emit(fmaR(-t2, sx, q.x + pwx), fmaR(-t2, sy, q.y + pwy),
+                     fmaR(-t2, sz, q.z + pwz), slot_base + nreg);
+            }
+        }
+    }
+    return nwall;
+}
+
+}  // namespace mps

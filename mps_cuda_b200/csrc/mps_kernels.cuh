@@ -1,0 +1,860 @@
+// mps_kernels.cuh -- sm_100a kernels of the explicit MPS step.
+//
+// Bucket build (replaces d_MkBkt's atomicExch linked list, kernel.cu:516-550):
+//   key   : bucket of every item, warp-aggregated atomicAdd on the bucket counter
+//   scan  : exclusive scan of the counters -> bucket start table (two launches)
+//   seg   : scatter ids into their bucket segment (arbitrary order inside a bucket)
+//   fin   : rank every item by id inside its bucket and gather its payload to the new slot
+// The result is deterministic: bucket-major, ascending id inside a bucket.
+//
+// Fused step (kernel.cu:1904-1935 in three neighbour passes):
+//   pass A: VscTrm + UpPcl1 (+ChkPcl)                            reads x^n, v^n, M1
+//   pass B: ChkCol + MkPrs + GenMRR/MRRinout at (x*, P)          reads x*, v*, walls, M1
+//   pass C: PrsGrdTrm + UpPcl2 (+ChkPcl) + GenMRR/MRRinout at (x^{n+1}, P)  reads x*, P, M2
+// Mirrors produced by pass C are the next step's first generation: GenMRR at the start of
+// the next step (kernel.cu:1906-1908) would read the same positions and pressures.
+#pragma once
+#include "mps_device.cuh"
+
+namespace mps {
+
+constexpr int kDiagCols = 11;
+enum { DG_CELL = 0, DG_VSC_F, DG_VSC_M, DG_COL_F, DG_COL_W, DG_COL_M, DG_PRS_F, DG_PRS_M,
+       DG_GRD_F, DG_GRD_M, DG_GEN_W };
+
+// ---------------------------------------------------------------------------------------
+// bucket build
+// ---------------------------------------------------------------------------------------
+template <class R, class RN> struct FluidKeySrc {
+    const SceneDev<R, RN>* sc;
+    int nscene, dead;
+    const V4<R>* pos;
+    const int8_t* typ;
+    const int* pid;
+    __device__ __forceinline__ int key(int t, DevCounters* cnt) const {
+        if (typ[t] != kFLD) return dead;
+        int id = pid[t];
+        int s = nscene > 1 ? scene_of(sc, nscene, id) : 0;
+        V4<R> p = pos[t];
+        if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) atomicAdd(&cnt->err_nan, 1);
+        int ix, iy, iz;
+        if (!cell_of(sc[s], p.x, p.y, p.z, ix, iy, iz)) atomicAdd(&cnt->err_cell, 1);
+        return sc[s].cbase + iz * sc[s].nbxy + iy * sc[s].nbx + ix;
+    }
+    __device__ __forceinline__ int id(int t) const { return pid[t]; }
+};
+
+template <class R, class RN> struct WallKeySrc {
+    const SceneDev<R, RN>* sc;
+    int nscene, dead;
+    const V4<R>* pos;
+    const int* wid;
+    __device__ __forceinline__ int key(int t, DevCounters* cnt) const {
+        int id = wid[t];
+        int s = nscene > 1 ? scene_of(sc, nscene, id) : 0;
+        V4<R> p = pos[t];
+        int ix, iy, iz;
+        if (!cell_of(sc[s], p.x, p.y, p.z, ix, iy, iz)) atomicAdd(&cnt->err_cell, 1);
+        return sc[s].cbase + iz * sc[s].nbxy + iy * sc[s].nbx + ix;
+    }
+    __device__ __forceinline__ int id(int t) const { return wid[t]; }
+};
+
+template <class R, class RN> struct MirrorKeySrc {
+    const SceneDev<R, RN>* sc;
+    int nscene, dead;
+    const V4<R>* pos;
+    const int* slot;
+    __device__ __forceinline__ int key(int t, DevCounters* cnt) const {
+        int sl = slot[t];
+        if (sl < 0) return dead;  // culled
+        int s = nscene > 1 ? scene_of(sc, nscene, sl / kNumMRR) : 0;
+        V4<R> p = pos[t];
+        int ix, iy, iz;
+        if (!cell_of(sc[s], p.x, p.y, p.z, ix, iy, iz)) atomicAdd(&cnt->err_cell, 1);
+        return sc[s].cbase + iz * sc[s].nbxy + iy * sc[s].nbx + ix;
+    }
+    __device__ __forceinline__ int id(int t) const { return slot[t]; }
+};
+
+__device__ __forceinline__ int item_count(const int* n_ptr, int n_fixed) {
+    return n_ptr ? min(*n_ptr, n_fixed) : n_fixed;
+}
+
+template <class Src>
+__global__ void k_bin_key(Src src, const int* n_ptr, int n_fixed, int* __restrict__ key,
+                          int* __restrict__ rnk, int* __restrict__ count, DevCounters* cnt) {
+    const int n = item_count(n_ptr, n_fixed);
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    // whole warps iterate together so that the warp-aggregated atomic sees every lane
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        int t = base + lane;
+        bool act = t < n;
+        int c = act ? src.key(t, cnt) : -1;
+        unsigned peers = __match_any_sync(0xffffffffu, c);
+        int leader = __ffs(peers) - 1;
+        int below = __popc(peers & ((1u << lane) - 1));
+        int b = 0;
+        if (act && lane == leader) b = atomicAdd(&count[c], __popc(peers));
+        b = __shfl_sync(0xffffffffu, b, leader);
+        if (act) {
+            key[t] = c;
+            rnk[t] = b + below;
+        }
+    }
+}
+
+template <class Src>
+__global__ void k_bin_seg(Src src, const int* n_ptr, int n_fixed, const int* __restrict__ key,
+                          const int* __restrict__ rnk, const int* __restrict__ cs,
+                          int* __restrict__ seg) {
+    const int n = item_count(n_ptr, n_fixed);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        seg[cs[key[t]] + rnk[t]] = src.id(t);
+}
+
+template <class Src, class G>
+__global__ void k_bin_fin(Src src, G g, const int* n_ptr, int n_fixed, const int* __restrict__ key,
+                          const int* __restrict__ rnk, const int* __restrict__ cs,
+                          const int* __restrict__ seg, int dead) {
+    const int n = item_count(n_ptr, n_fixed);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        int c = key[t];
+        int lo = __ldg(cs + c);
+        int d;
+        if (c == dead) {
+            d = lo + rnk[t];  // order of unlisted items is irrelevant
+        } else {
+            int hi = __ldg(cs + c + 1), my = src.id(t), r = 0;
+            for (int k = lo; k < hi; ++k) r += (__ldg(seg + k) < my);
+            d = lo + r;
+        }
+        g(t, d);
+    }
+}
+
+template <class R> struct FluidGather {
+    const V4<R>* pos; const V4<R>* vel; const V4<R>* acc;
+    const R* prs; const R* pav; const int* pid; const int8_t* typ;
+    V4<R>* dpos; V4<R>* dvel; V4<R>* dacc;
+    R* dprs; R* dpav; int* dpid; int8_t* dtyp;
+    __device__ __forceinline__ void operator()(int t, int d) const {
+        int8_t ty = typ[t];
+        dpos[d] = pos[t];
+        dvel[d] = vel[t];
+        if (acc) dacc[d] = acc[t];
+        dprs[d] = ty == kFLD ? prs[t] : R(0);
+        dpav[d] = pav[t];
+        dpid[d] = pid[t];
+        dtyp[d] = ty;
+    }
+};
+
+template <class R> struct MirrorGather {
+    const V4<R>* pos; const int* slot;
+    V4<R>* dpos; int* dslot;
+    __device__ __forceinline__ void operator()(int t, int d) const {
+        dpos[d] = pos[t];
+        dslot[d] = slot[t];
+    }
+};
+
+template <class R> struct WallGather {
+    const V4<R>* pos; const V4<R>* nrm; const V4<R>* vel; const int* wid; const int8_t* typ;
+    V4<R>* dpos; V4<R>* dnrm; V4<R>* dvel; int* dwid; int8_t* dtyp;
+    __device__ __forceinline__ void operator()(int t, int d) const {
+        dpos[d] = pos[t];
+        dnrm[d] = nrm[t];
+        dvel[d] = vel[t];
+        dwid[d] = wid[t];
+        dtyp[d] = typ[t];
+    }
+};
+
+// exclusive scan of count[0..L) into out[0..L], out[L] = total
+constexpr int kScanThreads = 1024, kScanPer = 4, kScanTile = kScanThreads * kScanPer;
+
+__device__ __forceinline__ int block_sum(int v, int* sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    int t = 0;
+    if (threadIdx.x < 32) {
+        t = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0;
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) sh[0] = t;
+    __syncthreads();
+    int r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+static __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const int* __restrict__ in, int L,
+                                                              int* __restrict__ part) {
+    __shared__ int sh[32];
+    int base = blockIdx.x * kScanTile + threadIdx.x * kScanPer;
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) v += (base + k < L) ? in[base + k] : 0;
+    int s = block_sum(v, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+static __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int* __restrict__ in, int L,
+                                                             const int* __restrict__ part,
+                                                             int* __restrict__ out) {
+    __shared__ int sh[32];
+    __shared__ int wsum[32];
+    // offset of this tile = sum of the partials before it
+    int off = 0;
+    for (int b = threadIdx.x; b < (int)blockIdx.x; b += blockDim.x) off += part[b];
+    off = block_sum(off, sh);
+    int base = blockIdx.x * kScanTile + threadIdx.x * kScanPer;
+    int v[kScanPer], loc = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        v[k] = (base + k < L) ? in[base + k] : 0;
+        loc += v[k];
+    }
+    // inclusive warp scan of the thread sums
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int inc = loc;
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) wsum[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        int ws = lane < (blockDim.x >> 5) ? wsum[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, ws, o);
+            if (lane >= o) ws += y;
+        }
+        wsum[lane] = ws;  // inclusive over warps
+    }
+    __syncthreads();
+    int excl = off + (w > 0 ? wsum[w - 1] : 0) + inc - loc;
+#pragma unroll
+    for (int k = 0; k < kScanPer; ++k) {
+        if (base + k < L) out[base + k] = excl;
+        excl += v[k];
+    }
+    if (base <= L - 1 && L - 1 < base + kScanPer) out[L] = excl;  // thread holding the last item
+}
+
+// ---------------------------------------------------------------------------------------
+// neighbour passes
+// ---------------------------------------------------------------------------------------
+template <class R, class RN> struct PassArgs {
+    const SceneDev<R, RN>* sc;
+    int nscene, nF, dead, skip;
+    const int* cs;  // fluid bucket starts
+    // sorted state
+    V4<R>* pos; V4<R>* vel; V4<R>* acc; R* prs; R* pav; const int* pid; int8_t* typ;
+    // scratch in the same slot order
+    V4<R>* tpos; V4<R>* tvel; R* tprs; int8_t* ttyp;
+    WallView<R> wl;
+    MirrorView<R> m;
+    MirrorSink<R> out;
+    DevCounters* cnt;
+    int32_t* diag;
+    RN* ndens;
+    // neighbour list, neighbour-major: nb[k * nF + s] is the k-th neighbour of slot s in
+    // visiting order; nbcnt[s] its length (lists longer than nbK fall back to a scan)
+    int* nb;
+    int* nbcnt;
+    int nbK;
+};
+
+template <class R, class RN>
+__device__ __forceinline__ const SceneDev<R, RN>& scene_ref(const PassArgs<R, RN>& a, int pid) {
+    return a.sc[a.nscene > 1 ? scene_of(a.sc, a.nscene, pid) : 0];
+}
+
+#define MPS_INF_SKIP(a, v) ((a).skip ? (v) : R(INFINITY))
+
+// Phase 1 of a neighbour pass: the fluid neighbours j != s with d2 <= thr, in visiting
+// order, into the slot's list. Returns the neighbour count (may exceed nbK).
+template <class R, class RN>
+__device__ __forceinline__ int build_list(const PassArgs<R, RN>& a, const SceneDev<R, RN>& sc,
+                                          const RowCtx<R>& c, int s, R x, R y, R z, R thr, R B) {
+    int cnt = 0;
+    int* __restrict__ nb = a.nb;
+    const int nF = a.nF, K = a.nbK;
+    for_rows(sc, a.cs, c, B, [&](int j) {
+        if (j == s) return;
+        V4<R> q = ldg4(a.pos + j);
+        R dx = q.x - x, dy = q.y - y, dz = q.z - z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (d2 <= thr) {
+            if (cnt < K) nb[size_t(cnt) * nF + s] = j;
+            ++cnt;
+        }
+    });
+    return cnt;
+}
+
+// pass A: VscTrm (kernel.cu:1013-1119) + UpPcl1/ChkPcl (kernel.cu:1138-1149, 481-513)
+template <class R, class RN, bool DIAG>
+__global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF) return;
+    const int nalive = __ldg(a.cs + a.dead);
+    if (s >= nalive) {  // unlisted particles are carried over unchanged
+        a.tpos[s] = a.pos[s];
+        a.tvel[s] = a.vel[s];
+        a.ttyp[s] = a.typ[s];
+        return;
+    }
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    V4<R> p = ldg4(a.pos + s), v = ldg4(a.vel + s);
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    R sx = 0, sy = 0, sz = 0;
+    int cf = 0, cm = 0;
+    const int n = build_list(a, sc, c, s, p.x, p.y, p.z, sc.r_le, MPS_INF_SKIP(a, sc.skip_r));
+    if (n <= a.nbK) {
+        for (int k = 0; k < n; ++k) {
+            const int j = a.nb[size_t(k) * a.nF + s];
+            V4<R> q = ldg4(a.pos + j), u = ldg4(a.vel + j);
+            R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+            R d2 = dot3(dx, dy, dz, dx, dy, dz);
+            R d = sqrtR(d2);
+            R w = sc.two_l0 / (d2 * d);
+            sx = fmaR(u.x - v.x, w, sx);
+            sy = fmaR(u.y - v.y, w, sy);
+            sz = fmaR(u.z - v.z, w, sz);
+        }
+        cf = n;
+        visc_sum_mirrors(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.m, MPS_INF_SKIP(a, sc.skip_r), sx, sy,
+                         sz, cm);
+    } else {
+        visc_sum(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.cs, a.pos, a.vel, a.m,
+                 MPS_INF_SKIP(a, sc.skip_r), sx, sy, sz, cf, cm);
+    }
+    R ax = fmaR(sc.kn, sx, sc.g[0]), ay = fmaR(sc.kn, sy, sc.g[1]), az = fmaR(sc.kn, sz, sc.g[2]);
+    R ux = fmaR(ax, sc.dt, v.x), uy = fmaR(ay, sc.dt, v.y), uz = fmaR(az, sc.dt, v.z);
+    R x = fmaR(ux, sc.dt, p.x), y = fmaR(uy, sc.dt, p.y), z = fmaR(uz, sc.dt, p.z);
+    bool alive = chkpcl(sc, x, y, z, ux, uy, uz);
+    if (!alive) {
+        x = y = z = ux = uy = uz = R(0);
+        atomicAdd(&a.cnt->deleted, 1);
+    }
+    a.tpos[s] = V4<R>{x, y, z, R(0)};
+    a.tvel[s] = V4<R>{ux, uy, uz, R(0)};
+    a.ttyp[s] = alive ? int8_t(kFLD) : int8_t(kGST);
+    if (DIAG) {
+        int32_t* d = a.diag + size_t(pid) * kDiagCols;
+        d[DG_VSC_F] = cf;
+        d[DG_VSC_M] = cm;
+    }
+}
+
+// pass B: ChkCol (kernel.cu:1168-1287) + MkPrs (kernel.cu:1306-1411) at x*; leaves the
+// list of fluid neighbours inside max(rp, rlim) for pass C (same positions, same slots)
+template <class R, class RN, bool DIAG>
+__global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF) return;
+    const int nalive = __ldg(a.cs + a.dead);
+    if (s >= nalive) {
+        a.tvel[s] = a.vel[s];
+        a.tprs[s] = R(0);
+        return;
+    }
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    V4<R> p = ldg4(a.pos + s), v = ldg4(a.vel + s);
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    R wx = v.x, wy = v.y, wz = v.z;
+    RN ni = 0;
+    int cnt5[5] = {0, 0, 0, 0, 0};
+    const int n = build_list(a, sc, c, s, p.x, p.y, p.z, sc.list_thr, MPS_INF_SKIP(a, sc.skip_rc));
+    a.nbcnt[s] = n;
+    if (n <= a.nbK) {
+        for (int k = 0; k < n; ++k) {
+            const int j = a.nb[size_t(k) * a.nF + s];
+            V4<R> q = ldg4(a.pos + j);
+            R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+            R d2 = dot3(dx, dy, dz, dx, dy, dz);
+            if (d2 < sc.rlim2) {
+                V4<R> u = ldg4(a.vel + j);
+                col_hit(sc.colfac, v.x, v.y, v.z, u.x, u.y, u.z, dx, dy, dz, d2, wx, wy, wz);
+                ++cnt5[0];
+            }
+            if (d2 <= sc.rp_lt) {
+                dens_add(sc, d2, ni);
+                ++cnt5[3];
+            }
+        }
+        col_dens_walls_mirrors<R, RN, true, true>(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.wl, a.m,
+                                                  a.skip != 0, wx, wy, wz, ni, cnt5);
+    } else {
+        col_dens_sum<R, RN, true, true>(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.cs, a.pos,
+                                        a.vel, a.wl, a.m, a.skip != 0, wx, wy, wz, ni, cnt5);
+    }
+    R P = eos(sc, ni);
+    a.tvel[s] = V4<R>{wx, wy, wz, R(0)};
+    a.tprs[s] = P;
+    if (DIAG) {
+        int32_t* d = a.diag + size_t(pid) * kDiagCols;
+        d[DG_COL_F] = cnt5[0];
+        d[DG_COL_W] = cnt5[1];
+        d[DG_COL_M] = cnt5[2];
+        d[DG_PRS_F] = cnt5[3];
+        d[DG_PRS_M] = cnt5[4];
+        a.ndens[pid] = ni;
+    }
+}
+
+// pass C: PrsGrdTrm (kernel.cu:1651-1794) + UpPcl2/ChkPcl (kernel.cu:1815-1829), walking
+// the neighbour lists pass B left
+template <class R, class RN, bool DIAG>
+__global__ void __launch_bounds__(128) k_pass_c(PassArgs<R, RN> a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF) return;
+    const int nalive = __ldg(a.cs + a.dead);
+    if (s >= nalive) {
+        a.tpos[s] = a.pos[s];
+        a.ttyp[s] = a.typ[s];
+        return;
+    }
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    V4<R> p = ldg4(a.pos + s);
+    const R pi = a.tprs[s];
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    R sx = 0, sy = 0, sz = 0;
+    int cf = 0, cm = 0;
+    const int n = a.nbcnt[s];
+    if (n <= a.nbK) {
+        R pmin = pi;
+        for (int k = 0; k < n; ++k) {
+            const int j = a.nb[size_t(k) * a.nF + s];
+            V4<R> q = ldg4(a.pos + j);
+            R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+            R d2 = dot3(dx, dy, dz, dx, dy, dz);
+            if (d2 < sc.rp2) {
+                R pj = __ldg(a.tprs + j);
+                if (pj < pmin) pmin = pj;
+            }
+        }
+        for (int k = 0; k < n; ++k) {
+            const int j = a.nb[size_t(k) * a.nF + s];
+            V4<R> q = ldg4(a.pos + j);
+            R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+            R d2 = dot3(dx, dy, dz, dx, dy, dz);
+            if (d2 < sc.rp2) {
+                R d = sqrtR(d2);
+                R w = wei_grad(d, sc.rp) / d2;
+                R pw = (__ldg(a.tprs + j) - pmin) * w;
+                sx = fmaR(pw, dx, sx);
+                sy = fmaR(pw, dy, sy);
+                sz = fmaR(pw, dz, sz);
+                ++cf;
+            }
+        }
+        grad_sum_mirrors(sc, c, pid - sc.pbase, p.x, p.y, p.z, pmin, a.m, a.skip != 0, sx, sy, sz,
+                         cm);
+    } else {
+        grad_sum(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, pi, a.cs, a.pos, a.tprs, a.m,
+                 a.skip != 0, sx, sy, sz, cf, cm);
+    }
+    R ax = (sc.invro * sx) * sc.a3, ay = (sc.invro * sy) * sc.a3, az = (sc.invro * sz) * sc.a3;
+    V4<R> v = a.tvel[s];
+    R ux = fmaR(ax, sc.dt, v.x), uy = fmaR(ay, sc.dt, v.y), uz = fmaR(az, sc.dt, v.z);
+    R x = fmaR(ax * sc.dt, sc.dt, p.x), y = fmaR(ay * sc.dt, sc.dt, p.y),
+      z = fmaR(az * sc.dt, sc.dt, p.z);
+    a.pav[s] = a.pav[s] + pi;
+    bool alive = chkpcl(sc, x, y, z, ux, uy, uz);
+    if (!alive) {
+        x = y = z = ux = uy = uz = R(0);
+        atomicAdd(&a.cnt->deleted, 1);
+    }
+    a.tpos[s] = V4<R>{x, y, z, R(0)};
+    a.tvel[s] = V4<R>{ux, uy, uz, R(0)};
+    a.ttyp[s] = alive ? int8_t(kFLD) : int8_t(kGST);
+    if (DIAG) {
+        int32_t* d = a.diag + size_t(pid) * kDiagCols;
+        d[DG_GRD_F] = cf;
+        d[DG_GRD_M] = cm;
+    }
+}
+
+// GenMRR_nonslip + MRRinout for every FLD slot of (gpos, gprs, gtyp): the second generation
+// of a step (x*, P after pass B) and the first generation of the next one (x^{n+1}, P after
+// pass C). Near-wall particles are a thin layer, so this runs as a light kernel of its own
+// instead of stretching the neighbour passes.
+template <class R, class RN>
+__global__ void __launch_bounds__(128) k_gen_cull(PassArgs<R, RN> a, const V4<R>* gpos,
+                                                  const R* gprs, const int8_t* gtyp) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF || gtyp[s] != kFLD) return;
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    V4<R> p = gpos[s];
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    gen_mirrors<R, RN, true>(sc, c, p.x, p.y, p.z, gprs[s], pid * kNumMRR, a.wl, a.skip != 0,
+                             a.out, a.cnt);
+}
+
+// ---------------------------------------------------------------------------------------
+// one reference method per launch (mps_phase); state is updated in place like the
+// reference's device arrays
+// ---------------------------------------------------------------------------------------
+template <class R, class RN, bool DIAG>
+__global__ void __launch_bounds__(128) k_ph_vsc(PassArgs<R, RN> a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF || a.typ[s] != kFLD) return;
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    V4<R> p = ldg4(a.pos + s), v = ldg4(a.vel + s);
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    R sx = 0, sy = 0, sz = 0;
+    int cf = 0, cm = 0;
+    visc_sum(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.cs, a.pos, a.vel, a.m,
+             MPS_INF_SKIP(a, sc.skip_r), sx, sy, sz, cf, cm);
+    a.acc[s] = V4<R>{fmaR(sc.kn, sx, sc.g[0]), fmaR(sc.kn, sy, sc.g[1]), fmaR(sc.kn, sz, sc.g[2]),
+                     R(0)};
+    if (DIAG) {
+        int32_t* d = a.diag + size_t(pid) * kDiagCols;
+        d[DG_VSC_F] = cf;
+        d[DG_VSC_M] = cm;
+    }
+}
+
+template <class R, class RN>
+__global__ void k_ph_uppcl1(PassArgs<R, RN> a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF || a.typ[s] != kFLD) return;
+    const SceneDev<R, RN>& sc = scene_ref(a, a.pid[s]);
+    V4<R> p = a.pos[s], v = a.vel[s], ac = a.acc[s];
+    R ux = fmaR(ac.x, sc.dt, v.x), uy = fmaR(ac.y, sc.dt, v.y), uz = fmaR(ac.z, sc.dt, v.z);
+    R x = fmaR(ux, sc.dt, p.x), y = fmaR(uy, sc.dt, p.y), z = fmaR(uz, sc.dt, p.z);
+    if (chkpcl(sc, x, y, z, ux, uy, uz)) {
+        a.pos[s] = V4<R>{x, y, z, R(0)};
+        a.vel[s] = V4<R>{ux, uy, uz, R(0)};
+    } else {
+        a.typ[s] = kGST;
+        a.pos[s] = V4<R>{0, 0, 0, 0};
+        a.vel[s] = V4<R>{0, 0, 0, 0};
+        a.prs[s] = R(0);
+        atomicAdd(&a.cnt->deleted, 1);
+    }
+    a.acc[s] = V4<R>{0, 0, 0, 0};
+}
+
+template <class R, class RN, bool DIAG>
+__global__ void __launch_bounds__(128) k_ph_col(PassArgs<R, RN> a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF || a.typ[s] != kFLD) return;
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    V4<R> p = ldg4(a.pos + s), v = ldg4(a.vel + s);
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    R wx = v.x, wy = v.y, wz = v.z;
+    RN ni = 0;
+    int cnt5[5] = {0, 0, 0, 0, 0};
+    col_dens_sum<R, RN, true, false>(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.cs, a.pos, a.vel,
+                                     a.wl, a.m, a.skip != 0, wx, wy, wz, ni, cnt5);
+    a.tvel[s] = V4<R>{wx, wy, wz, R(0)};
+    if (DIAG) {
+        int32_t* d = a.diag + size_t(pid) * kDiagCols;
+        d[DG_COL_F] = cnt5[0];
+        d[DG_COL_W] = cnt5[1];
+        d[DG_COL_M] = cnt5[2];
+    }
+}
+
+// d_UpChkCol (kernel.cu:1281-1287): Acc holds the corrected velocity, Vel = Acc
+template <class R, class RN>
+__global__ void k_ph_upchkcol(PassArgs<R, RN> a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF || a.typ[s] != kFLD) return;
+    V4<R> w = a.tvel[s];
+    a.acc[s] = w;
+    a.vel[s] = w;
+}
+
+template <class R, class RN, bool DIAG>
+__global__ void __launch_bounds__(128) k_ph_prs(PassArgs<R, RN> a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF || a.typ[s] != kFLD) return;
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    V4<R> p = ldg4(a.pos + s);
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    R wx = 0, wy = 0, wz = 0;
+    RN ni = 0;
+    int cnt5[5] = {0, 0, 0, 0, 0};
+    col_dens_sum<R, RN, false, true>(sc, c, s, p.x, p.y, p.z, R(0), R(0), R(0), a.cs, a.pos,
+                                     a.vel, a.wl, a.m, a.skip != 0, wx, wy, wz, ni, cnt5);
+    a.prs[s] = eos(sc, ni);
+    if (DIAG) {
+        int32_t* d = a.diag + size_t(pid) * kDiagCols;
+        d[DG_PRS_F] = cnt5[3];
+        d[DG_PRS_M] = cnt5[4];
+        a.ndens[pid] = ni;
+    }
+}
+
+template <class R, class RN, bool DIAG>
+__global__ void __launch_bounds__(128) k_ph_grd(PassArgs<R, RN> a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF || a.typ[s] != kFLD) return;
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    V4<R> p = ldg4(a.pos + s);
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    R sx = 0, sy = 0, sz = 0;
+    int cf = 0, cm = 0;
+    grad_sum(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, a.prs[s], a.cs, a.pos, a.prs, a.m,
+             a.skip != 0, sx, sy, sz, cf, cm);
+    a.acc[s] = V4<R>{(sc.invro * sx) * sc.a3, (sc.invro * sy) * sc.a3, (sc.invro * sz) * sc.a3,
+                     R(0)};
+    if (DIAG) {
+        int32_t* d = a.diag + size_t(pid) * kDiagCols;
+        d[DG_GRD_F] = cf;
+        d[DG_GRD_M] = cm;
+    }
+}
+
+template <class R, class RN>
+__global__ void k_ph_uppcl2(PassArgs<R, RN> a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF) return;
+    if (a.typ[s] == kFLD) {
+        const SceneDev<R, RN>& sc = scene_ref(a, a.pid[s]);
+        V4<R> p = a.pos[s], v = a.vel[s], ac = a.acc[s];
+        R ux = fmaR(ac.x, sc.dt, v.x), uy = fmaR(ac.y, sc.dt, v.y), uz = fmaR(ac.z, sc.dt, v.z);
+        R x = fmaR(ac.x * sc.dt, sc.dt, p.x), y = fmaR(ac.y * sc.dt, sc.dt, p.y),
+          z = fmaR(ac.z * sc.dt, sc.dt, p.z);
+        a.acc[s] = V4<R>{0, 0, 0, 0};
+        a.pav[s] = a.pav[s] + a.prs[s];
+        if (chkpcl(sc, x, y, z, ux, uy, uz)) {
+            a.pos[s] = V4<R>{x, y, z, R(0)};
+            a.vel[s] = V4<R>{ux, uy, uz, R(0)};
+        } else {
+            a.typ[s] = kGST;
+            a.pos[s] = V4<R>{0, 0, 0, 0};
+            a.vel[s] = V4<R>{0, 0, 0, 0};
+            a.prs[s] = R(0);
+            atomicAdd(&a.cnt->deleted, 1);
+        }
+    } else {
+        a.pav[s] = a.pav[s] + a.prs[s];
+    }
+}
+
+// GenMRR_nonslip without the cull (the cull is MkBkt_MRR's d_MRRinout)
+template <class R, class RN, bool DIAG>
+__global__ void __launch_bounds__(128) k_ph_gen(PassArgs<R, RN> a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF || a.typ[s] != kFLD) return;
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    V4<R> p = ldg4(a.pos + s);
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    int nw = gen_mirrors<R, RN, false>(sc, c, p.x, p.y, p.z, a.prs[s], pid * kNumMRR, a.wl,
+                                       a.skip != 0, a.out, a.cnt);
+    if (DIAG) a.diag[size_t(pid) * kDiagCols + DG_GEN_W] = nw;
+}
+
+// d_MRRinout over the raw mirrors; a culled mirror's slot becomes negative
+template <class R, class RN>
+__global__ void k_ph_cull(PassArgs<R, RN> a) {
+    const int n = min(a.cnt->mirror_raw, a.out.cap);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        int sl = a.out.slot[t];
+        if (sl < 0) continue;
+        const SceneDev<R, RN>& sc = a.sc[a.nscene > 1 ? scene_of(a.sc, a.nscene, sl / kNumMRR) : 0];
+        V4<R> q = a.out.pos[t];
+        if (!cull_keep(sc, q.x, q.y, q.z, a.wl, a.skip != 0, &a.cnt->err_cell))
+            a.out.slot[t] = -1 - sl;
+    }
+}
+
+// d_Surface_Edge (kernel.cu:553-668) over the sorted walls
+template <class R, class RN>
+__global__ void k_surface_edge(const SceneDev<R, RN>* scs, int nscene, int nW, WallView<R> wl,
+                               const int* wid, int8_t* wse) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nW) return;
+    const SceneDev<R, RN>& sc = scs[nscene > 1 ? scene_of(scs, nscene, wid[t]) : 0];
+    V4<R> p = wl.pos[t], n = wl.nrm[t];
+    int8_t ty = wl.typ[t];
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    bool edge = false;
+    for_rows(sc, wl.cs, c, R(INFINITY), [&](int j) {
+        if (j == t || wl.typ[j] != ty) return;
+        V4<R> q = wl.pos[j];
+        R dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (d2 < sc.edge_r2) {
+            V4<R> m = wl.nrm[j];
+            if (m.x != n.x || m.y != n.y || m.z != n.z) edge = true;
+        }
+    });
+    wse[t] = edge ? int8_t(kEDGE) : int8_t(0);
+}
+
+// ---------------------------------------------------------------------------------------
+// state transfer between id order (host layout) and slot order
+// ---------------------------------------------------------------------------------------
+template <class R> struct IdState {  // SoA, id order, n = all particles
+    int n;
+    R* pos; R* vel; R* acc; R* prs; R* pav; int8_t* typ;
+    int* cell;  // bucket index ib of the current position, -1 for GST
+};
+
+template <class R, class RN>
+__device__ __forceinline__ int local_cell(const SceneDev<R, RN>& sc, R x, R y, R z) {
+    int ix = int((x - sc.minc[0]) * sc.dbinv) + 1;
+    int iy = int((y - sc.minc[1]) * sc.dbinv) + 1;
+    int iz = int((z - sc.minc[2]) * sc.dbinv) + 1;
+    return iz * sc.nbxy + iy * sc.nbx + ix;
+}
+
+template <class R>
+__global__ void k_load_fluid(IdState<R> st, const int* fluid_ids, int nF, V4<R>* pos, V4<R>* vel,
+                             V4<R>* acc, R* prs, R* pav, int* pid, int8_t* typ, int use_acc) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nF) return;
+    const int id = fluid_ids[f];
+    const size_t n = st.n;
+    pos[f] = V4<R>{st.pos[id], st.pos[n + id], st.pos[2 * n + id], R(0)};
+    vel[f] = V4<R>{st.vel[id], st.vel[n + id], st.vel[2 * n + id], R(0)};
+    acc[f] = use_acc ? V4<R>{st.acc[id], st.acc[n + id], st.acc[2 * n + id], R(0)}
+                     : V4<R>{0, 0, 0, 0};
+    prs[f] = st.prs[id];
+    pav[f] = st.pav[id];
+    pid[f] = id;
+    typ[f] = st.typ[id] == kFLD ? int8_t(kFLD) : int8_t(kGST);
+}
+
+template <class R>
+__global__ void k_load_walls(int n, const R* pos, const R* vel, const R* nrm, const int8_t* ty,
+                             const int* wall_ids, int nW, V4<R>* wpos, V4<R>* wvel, V4<R>* wnrm,
+                             int* wid, int8_t* wtyp) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nW) return;
+    const int id = wall_ids[w];
+    const size_t N = n;
+    wpos[w] = V4<R>{pos[id], pos[N + id], pos[2 * N + id], R(0)};
+    wvel[w] = V4<R>{vel[id], vel[N + id], vel[2 * N + id], R(0)};
+    wnrm[w] = V4<R>{nrm[id], nrm[N + id], nrm[2 * N + id], R(0)};
+    wid[w] = id;
+    wtyp[w] = ty[id];
+}
+
+template <class R, class RN>
+__global__ void k_store_fluid(IdState<R> st, const SceneDev<R, RN>* scs, int nscene, int nF,
+                              const V4<R>* pos, const V4<R>* vel, const V4<R>* acc, const R* prs,
+                              const R* pav, const int* pid, const int8_t* typ) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nF) return;
+    const int id = pid[s];
+    if (st.cell) {
+        const SceneDev<R, RN>& sc = scs[nscene > 1 ? scene_of(scs, nscene, id) : 0];
+        st.cell[id] = typ[s] == kFLD ? local_cell(sc, pos[s].x, pos[s].y, pos[s].z) : -1;
+    }
+    const size_t n = st.n;
+    V4<R> p = pos[s], v = vel[s], a = acc[s];
+    st.pos[id] = p.x; st.pos[n + id] = p.y; st.pos[2 * n + id] = p.z;
+    st.vel[id] = v.x; st.vel[n + id] = v.y; st.vel[2 * n + id] = v.z;
+    st.acc[id] = a.x; st.acc[n + id] = a.y; st.acc[2 * n + id] = a.z;
+    st.prs[id] = prs[s];
+    st.pav[id] = pav[s];
+    st.typ[id] = typ[s];
+}
+
+template <class R, class RN>
+__global__ void k_store_walls(IdState<R> st, const SceneDev<R, RN>* scs, int nscene, int nW,
+                              const V4<R>* pos, const V4<R>* vel, const int* wid,
+                              const int8_t* wtyp) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nW) return;
+    const int id = wid[w];
+    if (st.cell) {
+        const SceneDev<R, RN>& sc = scs[nscene > 1 ? scene_of(scs, nscene, id) : 0];
+        st.cell[id] = local_cell(sc, pos[w].x, pos[w].y, pos[w].z);
+    }
+    const size_t n = st.n;
+    V4<R> p = pos[w], v = vel[w];
+    st.pos[id] = p.x; st.pos[n + id] = p.y; st.pos[2 * n + id] = p.z;
+    st.vel[id] = v.x; st.vel[n + id] = v.y; st.vel[2 * n + id] = v.z;
+    st.acc[id] = R(0); st.acc[n + id] = R(0); st.acc[2 * n + id] = R(0);
+    st.prs[id] = R(0);
+    st.pav[id] = R(0);
+    st.typ[id] = wtyp[w];
+}
+
+// per-scene integrals over the listed fluid slots [cs[cbase], cs[cbase + nbxyz])
+__device__ __forceinline__ void atomic_max_double(double* a, double v) {
+    unsigned long long* p = reinterpret_cast<unsigned long long*>(a);
+    unsigned long long old = *p;
+    while (__longlong_as_double((long long)old) < v) {
+        unsigned long long prev = atomicCAS(p, old, (unsigned long long)__double_as_longlong(v));
+        if (prev == old) break;
+        old = prev;
+    }
+}
+
+template <class R, class RN>
+__global__ void k_integrals(const SceneDev<R, RN>* scs, const int* cs, const V4<R>* pos,
+                            const V4<R>* vel, const int8_t* typ, const int* nbxyz, double* out) {
+    const int sidx = blockIdx.y;
+    const SceneDev<R, RN>& sc = scs[sidx];
+    const int lo = cs[sc.cbase], hi = cs[sc.cbase + nbxyz[sidx]];
+    double cx = 0, cy = 0, cz = 0, ke = 0, fr = -1e300, n = 0;
+    for (int s = lo + blockIdx.x * blockDim.x + threadIdx.x; s < hi; s += gridDim.x * blockDim.x) {
+        if (typ[s] != kFLD) continue;
+        V4<R> p = pos[s], v = vel[s];
+        cx += double(p.x); cy += double(p.y); cz += double(p.z);
+        ke += 0.5 * (double(v.x) * double(v.x) + double(v.y) * double(v.y) + double(v.z) * double(v.z));
+        fr = fmax(fr, double(p.x));
+        n += 1;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        cx += __shfl_down_sync(0xffffffffu, cx, o);
+        cy += __shfl_down_sync(0xffffffffu, cy, o);
+        cz += __shfl_down_sync(0xffffffffu, cz, o);
+        ke += __shfl_down_sync(0xffffffffu, ke, o);
+        n += __shfl_down_sync(0xffffffffu, n, o);
+        fr = fmax(fr, __shfl_down_sync(0xffffffffu, fr, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        double* o = out + 6 * sidx;
+        atomicAdd(o + 0, cx); atomicAdd(o + 1, cy); atomicAdd(o + 2, cz);
+        atomicAdd(o + 3, ke); atomicAdd(o + 5, n);
+        if (n > 0) atomic_max_double(o + 4, fr);
+    }
+}
+
+}  // namespace mps

@@ -1,0 +1,812 @@
+// mps_solver.cuh -- host side of the B200 MPS solver (templated on the arithmetic).
+//
+// One handle owns the device state of one or more scenes. The reference keeps that state
+// in public members of `class MPS` (class.cuh:49-141) and drives it from ClcMPS
+// (kernel.cu:1872-1943) with a blocking cudaDeviceSynchronize after every kernel; here the
+// whole step is queued on one stream (optionally replayed as a CUDA graph) and nothing
+// synchronises until the caller reads data back.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/mps_b200.h"
+#include "mps_kernels.cuh"
+
+namespace mps {
+
+extern thread_local std::string g_last_error;
+
+struct ApiError : std::runtime_error {
+    int code;
+    ApiError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(call)                                                                             \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            throw ApiError(e_ == cudaErrorMemoryAllocation ? MPS_ERR_NOMEM : MPS_ERR_CUDA,   \
+                           std::string(#call) + ": " + cudaGetErrorString(e_));              \
+        }                                                                                    \
+    } while (0)
+
+#define CKL() CK(cudaGetLastError())
+
+// ---- derived constants (AlcBkt + SetPara, kernel.cu:307-415) ----------------------------
+template <class R> static R wei(R d, R re) { return ((re / d) + (d / re)) - R(2); }
+template <class R> static R wei_grad_h(R d, R re) { return (re / d) - (d / re); }
+
+// largest t with sqrt(t) <= r (le = true) or sqrt(t) < r (le = false), so that
+// `sqrt(d2) <= r` can be tested as `d2 <= t` without a square root
+template <class R> static R sqrt_threshold(R r, bool le) {
+    auto ok = [&](R t) { R s = std::sqrt(t); return le ? (s <= r) : (s < r); };
+    R t = r * r;
+    while (!ok(t)) t = std::nextafter(t, R(0));
+    for (;;) {
+        R u = std::nextafter(t, R(INFINITY));
+        if (!ok(u)) break;
+        t = u;
+    }
+    return t;
+}
+
+template <class R, class RN>
+static void derive_scene(const mps_params& p, int cbase, int pbase, int pcount, SceneDev<R, RN>& s,
+                         mps_info& inf) {
+    std::memset(&s, 0, sizeof(s));
+    const R l0 = R(p.pcl_dst);
+    R maxc[3];
+    for (int d = 0; d < 3; ++d) {
+        s.minc[d] = R(double(R(p.min[d])) - 3.1 * double(l0));  // kernel.cu:26-31
+        maxc[d] = R(double(R(p.max[d])) + 3.1 * double(l0));
+        s.g[d] = R(p.g[d]);
+    }
+    const R r = l0 * R(3.1), r2 = r * r, rp = l0 * R(2.1), rp2 = rp * rp;
+    const R db = l0 * R(3.1), dbinv = R(1) / db;
+    s.db = db;
+    s.dbinv = dbinv;
+    s.nbx = int((maxc[0] - s.minc[0]) * dbinv) + 3;  // kernel.cu:317-319
+    s.nby = int((maxc[1] - s.minc[1]) * dbinv) + 3;
+    s.nbz = int((maxc[2] - s.minc[2]) * dbinv) + 3;
+    s.nbxy = s.nbx * s.nby;
+    s.cbase = cbase;
+    s.pbase = pbase;
+    s.pcount = pcount;
+    // lattice sums, kernel.cu:336-366
+    R tn0 = 0, tn0g = 0, tl = 0, tlg = 0;
+    int cnt = 0;
+    for (int ix = -10; ix < 10; ++ix)
+        for (int iy = -10; iy < 10; ++iy)
+            for (int iz = -10; iz < 10; ++iz) {
+                R x = l0 * R(ix), y = l0 * R(iy), z = l0 * R(iz);
+                R d2 = x * x + y * y + z * z;
+                if (d2 == R(0)) continue;
+                R d = std::sqrt(d2);
+                if (d2 < rp2) {
+                    tn0g += wei_grad_h(d, rp);
+                    tlg += d2 * wei_grad_h(d, rp);
+                    cnt += 1;
+                }
+                if (d2 < r2) {
+                    tn0 += wei(d, r);
+                    tl += d2 * wei(d, r);
+                }
+            }
+    const R n0 = tn0, n0_grad = tn0g;
+    const R rlim = l0 * R(p.dst_lmt_rat), rlim2 = rlim * rlim;  // kernel.cu:370-371
+    const R col = R(p.col_rat) + R(1);                           // kernel.cu:373
+    const R rho = R(p.rho), knm = R(p.knm_vsc), snd = R(p.snd);
+    const R rw = R(0.45) * l0;  // kernel.cu:1184
+    s.r = r; s.r2 = r2; s.r_le = sqrt_threshold(r, true);
+    s.rp = rp; s.rp2 = rp2; s.rp_lt = sqrt_threshold(rp, false);
+    s.rlim2 = rlim2;
+    // one list serves dist2 < rlim2 (ChkCol), sqrt(dist2) < rp (MkPrs), dist2 < rp2 (PrsGrdTrm)
+    s.list_thr = std::max({std::nextafter(rlim2, R(0)), s.rp_lt, std::nextafter(rp2, R(0))});
+    s.rlimw2 = rw * rw;
+    s.edge_r2 = (R(1) * l0) * (R(1) * l0);
+    s.wall_dist0 = R(10) * r;
+    s.two_l0 = R(2) * l0;
+    s.kn = (R(1) / n0) * knm;
+    s.dt = R(p.dt);
+    s.umax = R(p.umax);
+    for (int d = 0; d < 3; ++d) {
+        R t = R(3.1) * l0;
+        s.lo[d] = s.minc[d] + t;
+        s.hi[d] = maxc[d] - t;
+    }
+    s.colfac = (col * rho) / (rho + rho);
+    s.invro = R(-1) / rho;
+    s.a3 = R(3) / n0_grad;
+    const double m = 1e-3 * double(db);
+    auto sq = [&](double v) { return R((v + m) * (v + m)); };
+    s.skip_r = sq(double(r));
+    s.skip_rp = sq(double(rp));
+    s.skip_rl = sq(double(rlim));
+    s.skip_rw = sq(double(rw));
+    s.skip_rc = sq(std::max(double(rlim), double(rp)));
+    // number density / EOS arithmetic
+    RN n0g;
+    if (sizeof(RN) == sizeof(R)) {
+        n0g = RN(n0_grad);
+    } else {
+        RN acc = 0, l0n = RN(l0), rpn = RN(rp), rp2n = rpn * rpn;
+        for (int ix = -10; ix < 10; ++ix)
+            for (int iy = -10; iy < 10; ++iy)
+                for (int iz = -10; iz < 10; ++iz) {
+                    RN x = l0n * RN(ix), y = l0n * RN(iy), z = l0n * RN(iz);
+                    RN d2 = x * x + y * y + z * z;
+                    if (d2 == RN(0)) continue;
+                    if (d2 < rp2n) acc += wei_grad_h(RN(std::sqrt(d2)), rpn);
+                }
+        n0g = acc;
+    }
+    s.n0g = n0g;
+    s.prs_coef = RN(snd) * RN(snd) / n0g;  // kernel.cu:409
+    s.pmax = RN(R(p.pmax));
+    s.rho = RN(rho);
+    s.rp_n = RN(rp);
+
+    std::memset(&inf, 0, sizeof(inf));
+    inf.nbx = s.nbx; inf.nby = s.nby; inf.nbz = s.nbz; inf.nbxyz = s.nbxy * s.nbz;
+    inf.r = r; inf.rp = rp; inf.db = db; inf.dbinv = dbinv;
+    inf.n0 = n0; inf.lmd = tl / tn0; inf.n0_grad = n0_grad; inf.lmd_grad = tlg / tn0g;
+    inf.numn0_grad = cnt;
+    inf.rlim2 = rlim2; inf.col = col; inf.prs_coef = double(s.prs_coef); inf.pmax = double(s.pmax);
+    inf.umax = s.umax; inf.dt = s.dt; inf.snd = snd;
+    for (int d = 0; d < 3; ++d) { inf.minc[d] = s.minc[d]; inf.maxc[d] = maxc[d]; }
+}
+
+// ---- device allocation ---------------------------------------------------------------------
+struct DevArena {
+    std::vector<void*> ptrs;
+    template <class T> T* get(size_t n) {
+        void* p = nullptr;
+        size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw ApiError(MPS_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+        }
+        ptrs.push_back(p);
+        return static_cast<T*>(p);
+    }
+    ~DevArena() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+};
+
+template <class R> struct FluidBuf {
+    V4<R>* pos; V4<R>* vel; V4<R>* acc; R* prs; R* pav; int* pid; int8_t* typ;
+};
+template <class R> struct MirrorBuf {
+    V4<R>* pos; int* slot;
+};
+
+struct SolverBase {
+    virtual ~SolverBase() {}
+    int dev = 0;
+    cudaStream_t stream = 0, own_stream = 0;
+    int nscene = 0, nT = 0, nF = 0, nW = 0, C = 0, cap = 0;
+    int precision = 0;
+    std::vector<mps_info> infos;
+    std::vector<int> counts;
+    bool diag_on = false, graph_on = false;
+    int skip_opt = 1, block = 128;
+    long long steps = 0;
+    virtual void step(int n) = 0;
+    virtual void phase(int ph) = 0;
+    virtual void get_state(int8_t*, void*, void*, void*, void*, void*) = 0;
+    virtual void set_state(const int8_t*, const void*, const void*, const void*, const void*,
+                           const void*) = 0;
+    virtual void get_wall_flags(int8_t*) = 0;
+    virtual int get_mirrors(int which, int cap, int32_t* slot, void* pos, void* prs) = 0;
+    virtual void get_diag(int32_t* table, void* ndens) = 0;
+    virtual void get_counters(mps_counters*) = 0;
+    virtual void integrals(int scene, double out[6]) = 0;
+    virtual void invalidate_graph() = 0;
+};
+
+template <class R, class RN> class Solver final : public SolverBase {
+   public:
+    using SD = SceneDev<R, RN>;
+    DevArena ar;
+    std::vector<SD> hsc;
+    SD* d_sc = nullptr;
+    int* d_nbxyz = nullptr;
+    FluidBuf<R> S, S2;
+    V4<R>* t_pos; V4<R>* t_vel; R* t_prs; int8_t* t_typ;
+    // walls, sorted once
+    V4<R>* w_pos; V4<R>* w_nrm; V4<R>* w_vel; int* w_id; int8_t* w_typ; int8_t* w_se;
+    int* wcs;
+    // mirrors: raw list U and two sorted generations
+    MirrorBuf<R> U, M1, M2;
+    int *mcs1, *mcs2;
+    int* cs;
+    // bucket-build scratch
+    int *key, *rnk, *seg, *count, *part;
+    int* d_fluid_ids;
+    int* d_wall_ids;
+    int* d_nF;
+    DevCounters* cnt;
+    int32_t* diag;
+    RN* ndens;
+    IdState<R> io;
+    double* d_integ;
+    int* nb;
+    int* nbcnt;
+    int nbK = 160;  // list capacity: about 125 neighbours lie inside r at rest density
+    std::vector<int> fluid_ids, wall_ids;
+    bool lists_valid = false, sorted = false, m1_valid = false, acc_dirty = false;
+    cudaGraphExec_t gexec = nullptr;
+    bool gexec_diag = false;
+
+    ~Solver() override {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (own_stream) {
+            cudaStreamSynchronize(own_stream);
+            cudaStreamDestroy(own_stream);
+        }
+    }
+
+    int dead() const { return C; }
+    int L() const { return C + 1; }
+    int blocks(int n, int b) const { return std::max(1, (n + b - 1) / b); }
+
+    void init(int ns, const mps_params* p, const int32_t* cnts, const int8_t* typ_in,
+              const R* pos, const R* vel, const R* nrm) {
+        CK(cudaGetDevice(&dev));
+        // a stream of its own: the legacy default stream cannot be captured into a graph
+        CK(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+        stream = own_stream;
+        nscene = ns;
+        precision = p[0].precision;
+        counts.assign(cnts, cnts + ns);
+        nT = 0;
+        for (int s = 0; s < ns; ++s) nT += cnts[s];
+        hsc.resize(ns);
+        infos.resize(ns);
+        int cb = 0, pb = 0;
+        for (int s = 0; s < ns; ++s) {
+            derive_scene<R, RN>(p[s], cb, pb, cnts[s], hsc[s], infos[s]);
+            cb += infos[s].nbxyz;
+            pb += cnts[s];
+        }
+        C = cb;
+        // classify particles: walls inside the padded box are static walls, everything
+        // else is a fluid-class particle; RdDat drops what lies outside (kernel.cu:117)
+        std::vector<int8_t> ty(typ_in, typ_in + nT);
+        fluid_ids.clear();
+        wall_ids.clear();
+        for (int s = 0, id = 0; s < ns; ++s) {
+            R maxc[3];
+            for (int d = 0; d < 3; ++d) maxc[d] = R(infos[s].maxc[d]);
+            for (int k = 0; k < cnts[s]; ++k, ++id) {
+                R x = pos[id], y = pos[nT + id], z = pos[2 * size_t(nT) + id];
+                bool in = x < maxc[0] && x > hsc[s].minc[0] && y < maxc[1] && y > hsc[s].minc[1] &&
+                          z < maxc[2] && z > hsc[s].minc[2];
+                int t = ty[id];
+                if (t != kGST && t != kFLD && t != kWLL && t != kOBJ && t != kOBJ2)
+                    throw ApiError(MPS_ERR_ARG, "particle " + std::to_string(id) + " has type " +
+                                                    std::to_string(t));
+                bool wall = (t == kWLL || t == kOBJ || t == kOBJ2);
+                if (!in) ty[id] = kGST;
+                if (wall && in) wall_ids.push_back(id);
+                else fluid_ids.push_back(id);
+            }
+        }
+        nF = int(fluid_ids.size());
+        nW = int(wall_ids.size());
+        cap = std::max(1024, kNumMRR * nF);
+        allocate();
+        CK(cudaMemcpyAsync(d_sc, hsc.data(), sizeof(SD) * ns, cudaMemcpyHostToDevice, stream));
+        std::vector<int> nb(ns);
+        for (int s = 0; s < ns; ++s) nb[s] = infos[s].nbxyz;
+        CK(cudaMemcpyAsync(d_nbxyz, nb.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, stream));
+        if (nF > 0)
+            CK(cudaMemcpyAsync(d_fluid_ids, fluid_ids.data(), sizeof(int) * nF,
+                               cudaMemcpyHostToDevice, stream));
+        if (nW > 0)
+            CK(cudaMemcpyAsync(d_wall_ids, wall_ids.data(), sizeof(int) * nW,
+                               cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_nF, &nF, sizeof(int), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemsetAsync(cnt, 0, sizeof(DevCounters), stream));
+        CK(cudaMemsetAsync(diag, 0, sizeof(int32_t) * kDiagCols * size_t(nT), stream));
+        CK(cudaMemsetAsync(ndens, 0, sizeof(RN) * size_t(nT), stream));
+        // upload: nrm goes through the acc staging buffer
+        const size_t n3 = 3 * size_t(nT) * sizeof(R);
+        CK(cudaMemcpyAsync(io.pos, pos, n3, cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(io.vel, vel, n3, cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(io.acc, nrm, n3, cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(io.typ, ty.data(), nT, cudaMemcpyHostToDevice, stream));
+        CK(cudaMemsetAsync(io.prs, 0, sizeof(R) * nT, stream));
+        CK(cudaMemsetAsync(io.pav, 0, sizeof(R) * nT, stream));
+        if (nW > 0) {
+            // walls: unsorted copy in id order, then one bucket build into w_*
+            V4<R>* sp = ar.template get<V4<R>>(3 * size_t(nW));
+            V4<R>* tw_pos = sp;
+            V4<R>* tw_vel = sp + nW;
+            V4<R>* tw_nrm = sp + 2 * size_t(nW);
+            int8_t* tw_typ = ar.template get<int8_t>(nW);
+            int* tw_id = ar.template get<int>(nW);
+            k_load_walls<R><<<blocks(nW, 256), 256, 0, stream>>>(nT, io.pos, io.vel, io.acc, io.typ,
+                                                                 d_wall_ids, nW, tw_pos, tw_vel,
+                                                                 tw_nrm, tw_id, tw_typ);
+            CKL();
+            WallKeySrc<R, RN> ks{d_sc, nscene, dead(), tw_pos, tw_id};
+            WallGather<R> g{tw_pos, tw_nrm, tw_vel, tw_id, tw_typ, w_pos, w_nrm, w_vel, w_id, w_typ};
+            bin(ks, g, nullptr, nW, wcs);
+            WallView<R> wl = wall_view();
+            k_surface_edge<R, RN><<<blocks(nW, 128), 128, 0, stream>>>(d_sc, nscene, nW, wl, w_id,
+                                                                       w_se);
+            CKL();
+        } else {
+            CK(cudaMemsetAsync(wcs, 0, sizeof(int) * (L() + 1), stream));
+        }
+        load_fluid(false);
+        mkbkt(true);
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    void allocate() {
+        const size_t F = std::max(nF, 1), W = std::max(nW, 1), T = std::max(nT, 1);
+        d_sc = ar.template get<SD>(nscene);
+        d_nbxyz = ar.template get<int>(nscene);
+        for (FluidBuf<R>* b : {&S, &S2}) {
+            b->pos = ar.template get<V4<R>>(F);
+            b->vel = ar.template get<V4<R>>(F);
+            b->acc = ar.template get<V4<R>>(F);
+            b->prs = ar.template get<R>(F);
+            b->pav = ar.template get<R>(F);
+            b->pid = ar.template get<int>(F);
+            b->typ = ar.template get<int8_t>(F);
+        }
+        t_pos = ar.template get<V4<R>>(F);
+        t_vel = ar.template get<V4<R>>(F);
+        t_prs = ar.template get<R>(F);
+        t_typ = ar.template get<int8_t>(F);
+        w_pos = ar.template get<V4<R>>(W);
+        w_nrm = ar.template get<V4<R>>(W);
+        w_vel = ar.template get<V4<R>>(W);
+        w_id = ar.template get<int>(W);
+        w_typ = ar.template get<int8_t>(W);
+        w_se = ar.template get<int8_t>(W);
+        wcs = ar.template get<int>(L() + 1);
+        cs = ar.template get<int>(L() + 1);
+        for (MirrorBuf<R>* b : {&U, &M1, &M2}) {
+            b->pos = ar.template get<V4<R>>(cap);
+            b->slot = ar.template get<int>(cap);
+        }
+        mcs1 = ar.template get<int>(L() + 1);
+        mcs2 = ar.template get<int>(L() + 1);
+        const size_t items = std::max<size_t>({F, W, size_t(cap)});
+        key = ar.template get<int>(items);
+        rnk = ar.template get<int>(items);
+        seg = ar.template get<int>(items);
+        count = ar.template get<int>(L());
+        part = ar.template get<int>((L() + kScanTile - 1) / kScanTile + 1);
+        d_fluid_ids = ar.template get<int>(F);
+        d_wall_ids = ar.template get<int>(W);
+        d_nF = ar.template get<int>(1);
+        cnt = ar.template get<DevCounters>(1);
+        diag = ar.template get<int32_t>(kDiagCols * T);
+        ndens = ar.template get<RN>(T);
+        io.n = nT;
+        io.pos = ar.template get<R>(3 * T);
+        io.vel = ar.template get<R>(3 * T);
+        io.acc = ar.template get<R>(3 * T);
+        io.prs = ar.template get<R>(T);
+        io.pav = ar.template get<R>(T);
+        io.typ = ar.template get<int8_t>(T);
+        io.cell = ar.template get<int>(T);
+        d_integ = ar.template get<double>(6 * size_t(nscene));
+        nb = ar.template get<int>(size_t(nbK) * F);
+        nbcnt = ar.template get<int>(F);
+        CK(cudaMemsetAsync(S.acc, 0, sizeof(V4<R>) * F, stream));
+        CK(cudaMemsetAsync(S2.acc, 0, sizeof(V4<R>) * F, stream));
+        CK(cudaMemsetAsync(M1.slot, 0, sizeof(int) * cap, stream));
+        CK(cudaMemsetAsync(mcs1, 0, sizeof(int) * (L() + 1), stream));
+        CK(cudaMemsetAsync(mcs2, 0, sizeof(int) * (L() + 1), stream));
+    }
+
+    // ---- bucket build ------------------------------------------------------------------
+    template <class Src, class G> void bin(Src src, G g, const int* n_ptr, int n_max, int* out_cs) {
+        CK(cudaMemsetAsync(count, 0, sizeof(int) * L(), stream));
+        if (n_max > 0) {
+            int grid = std::min(blocks(n_max, 256), 148 * 32);
+            k_bin_key<Src><<<grid, 256, 0, stream>>>(src, n_ptr, n_max, key, rnk, count, cnt);
+            CKL();
+        }
+        int nb = (L() + kScanTile - 1) / kScanTile;
+        k_scan_reduce<<<nb, kScanThreads, 0, stream>>>(count, L(), part);
+        CKL();
+        k_scan_apply<<<nb, kScanThreads, 0, stream>>>(count, L(), part, out_cs);
+        CKL();
+        if (n_max > 0) {
+            int grid = std::min(blocks(n_max, 256), 148 * 32);
+            k_bin_seg<Src><<<grid, 256, 0, stream>>>(src, n_ptr, n_max, key, rnk, out_cs, seg);
+            CKL();
+            k_bin_fin<Src, G><<<grid, 256, 0, stream>>>(src, g, n_ptr, n_max, key, rnk, out_cs, seg,
+                                                        dead());
+            CKL();
+        }
+    }
+
+    // fluid bucket build from (pos, vel, typ) sources into S2, then S <-> S2
+    void bin_fluid(const V4<R>* pos, const V4<R>* vel, const V4<R>* acc, const R* prs,
+                   const R* pav, const int* pid, const int8_t* typ) {
+        FluidKeySrc<R, RN> ks{d_sc, nscene, dead(), pos, typ, pid};
+        FluidGather<R> g{pos, vel, acc, prs, pav, pid, typ,
+                         S2.pos, S2.vel, S2.acc, S2.prs, S2.pav, S2.pid, S2.typ};
+        bin(ks, g, nullptr, nF, cs);
+        std::swap(S, S2);
+    }
+
+    void mkbkt(bool with_acc) {
+        bin_fluid(S.pos, S.vel, with_acc ? S.acc : nullptr, S.prs, S.pav, S.pid, S.typ);
+        lists_valid = sorted = true;
+    }
+
+    void bin_mirrors(MirrorBuf<R>& dst, int* dcs) {
+        MirrorKeySrc<R, RN> ks{d_sc, nscene, dead(), U.pos, U.slot};
+        MirrorGather<R> g{U.pos, U.slot, dst.pos, dst.slot};
+        bin(ks, g, &cnt->mirror_raw, cap, dcs);
+    }
+
+    WallView<R> wall_view() const { return WallView<R>{wcs, w_pos, w_nrm, w_vel, w_se, w_typ}; }
+
+    PassArgs<R, RN> args(const MirrorBuf<R>& m, const int* mcs) {
+        PassArgs<R, RN> a;
+        a.sc = d_sc; a.nscene = nscene; a.nF = nF; a.dead = dead();
+        a.skip = (skip_opt && sorted) ? 1 : 0;
+        a.cs = cs;
+        a.pos = S.pos; a.vel = S.vel; a.acc = S.acc; a.prs = S.prs; a.pav = S.pav; a.pid = S.pid;
+        a.typ = S.typ;
+        a.tpos = t_pos; a.tvel = t_vel; a.tprs = t_prs; a.ttyp = t_typ;
+        a.wl = wall_view();
+        a.m = MirrorView<R>{mcs, m.pos, m.slot};
+        a.out = MirrorSink<R>{U.pos, U.slot, cap};
+        a.cnt = cnt; a.diag = diag; a.ndens = ndens;
+        a.nb = nb; a.nbcnt = nbcnt; a.nbK = nbK;
+        return a;
+    }
+
+    void reset_raw() { CK(cudaMemsetAsync(&cnt->mirror_raw, 0, sizeof(int), stream)); }
+
+    template <bool D> void fused_body() {
+        const int gb = blocks(nF, block);
+        // pass A: VscTrm + UpPcl1
+        k_pass_a<R, RN, D><<<gb, block, 0, stream>>>(args(M1, mcs1));
+        CKL();
+        // MkBkt on x* (kernel.cu:1917); the rebuild at kernel.cu:1921 would give the same lists
+        bin_fluid(t_pos, t_vel, nullptr, S.prs, S.pav, S.pid, t_typ);
+        // pass B: ChkCol + MkPrs, then the second mirror generation at (x*, P)
+        k_pass_b<R, RN, D><<<gb, block, 0, stream>>>(args(M1, mcs1));
+        CKL();
+        reset_raw();
+        k_gen_cull<R, RN><<<gb, block, 0, stream>>>(args(M1, mcs1), S.pos, t_prs, S.typ);
+        CKL();
+        bin_mirrors(M2, mcs2);
+        // pass C: PrsGrdTrm + UpPcl2, then the first mirror generation of the next step
+        k_pass_c<R, RN, D><<<gb, block, 0, stream>>>(args(M2, mcs2));
+        CKL();
+        reset_raw();
+        k_gen_cull<R, RN><<<gb, block, 0, stream>>>(args(M2, mcs2), t_pos, t_prs, t_typ);
+        CKL();
+        bin_fluid(t_pos, t_vel, nullptr, t_prs, S.pav, S.pid, t_typ);
+        bin_mirrors(M1, mcs1);
+    }
+
+    void prepare_fused() {
+        if (!lists_valid || !sorted) mkbkt(acc_dirty);
+        if (acc_dirty) {
+            CK(cudaMemsetAsync(S.acc, 0, sizeof(V4<R>) * std::max(nF, 1), stream));
+            CK(cudaMemsetAsync(S2.acc, 0, sizeof(V4<R>) * std::max(nF, 1), stream));
+            acc_dirty = false;
+        }
+        if (!m1_valid) {
+            reset_raw();
+            k_gen_cull<R, RN><<<blocks(nF, block), block, 0, stream>>>(args(M1, mcs1), S.pos, S.prs,
+                                                                       S.typ);
+            CKL();
+            bin_mirrors(M1, mcs1);
+            m1_valid = true;
+        }
+    }
+
+    void run_body() {
+        if (diag_on) fused_body<true>(); else fused_body<false>();
+    }
+
+    void invalidate_graph() override {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+    }
+
+    void step(int n) override {
+        if (n <= 0) return;
+        int done = 0;
+        if (!(lists_valid && sorted && m1_valid) || acc_dirty) {
+            prepare_fused();
+            run_body();
+            ++done;
+        }
+        if (graph_on && n - done > 0) {
+            if (gexec && gexec_diag != diag_on) invalidate_graph();
+            if (!gexec) {
+                cudaGraph_t g;
+                CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                try {
+                    run_body();
+                } catch (...) {
+                    cudaStreamEndCapture(stream, &g);
+                    throw;
+                }
+                CK(cudaStreamEndCapture(stream, &g));
+                cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+                cudaGraphDestroy(g);
+                CK(e);
+                gexec_diag = diag_on;
+            }
+            for (; done < n; ++done) CK(cudaGraphLaunch(gexec, stream));
+        } else {
+            for (; done < n; ++done) run_body();
+        }
+        steps += n;
+        lists_valid = sorted = m1_valid = true;
+    }
+
+    void phase(int ph) override {
+        PassArgs<R, RN> a = args(M1, mcs1);
+        const int gb = blocks(nF, block);
+        auto need_lists = [&]() {
+            if (!lists_valid)
+                throw ApiError(MPS_ERR_STATE, "bucket lists are not built: run MPS_PHASE_MKBKT first");
+        };
+        m1_valid = false;
+        switch (ph) {
+            case MPS_PHASE_MKBKT:
+                mkbkt(true);
+                break;
+            case MPS_PHASE_SURFACE_EDGE:
+                if (nW > 0) {
+                    k_surface_edge<R, RN><<<blocks(nW, 128), 128, 0, stream>>>(d_sc, nscene, nW,
+                                                                               wall_view(), w_id, w_se);
+                    CKL();
+                }
+                break;
+            case MPS_PHASE_RESETMRR:
+                reset_raw();
+                break;
+            case MPS_PHASE_GENMRR_NONSLIP:
+                if (diag_on) k_ph_gen<R, RN, true><<<gb, block, 0, stream>>>(a);
+                else k_ph_gen<R, RN, false><<<gb, block, 0, stream>>>(a);
+                CKL();
+                break;
+            case MPS_PHASE_MKBKT_MRR:
+                k_ph_cull<R, RN><<<std::min(blocks(cap, 256), 148 * 16), 256, 0, stream>>>(a);
+                CKL();
+                bin_mirrors(M1, mcs1);
+                break;
+            case MPS_PHASE_VSCTRM:
+                need_lists();
+                if (diag_on) k_ph_vsc<R, RN, true><<<gb, block, 0, stream>>>(a);
+                else k_ph_vsc<R, RN, false><<<gb, block, 0, stream>>>(a);
+                CKL();
+                acc_dirty = true;
+                break;
+            case MPS_PHASE_UPPCL1:
+                k_ph_uppcl1<R, RN><<<gb, block, 0, stream>>>(a);
+                CKL();
+                sorted = false;
+                acc_dirty = true;
+                break;
+            case MPS_PHASE_CHKCOL:
+                need_lists();
+                if (diag_on) k_ph_col<R, RN, true><<<gb, block, 0, stream>>>(a);
+                else k_ph_col<R, RN, false><<<gb, block, 0, stream>>>(a);
+                CKL();
+                k_ph_upchkcol<R, RN><<<gb, block, 0, stream>>>(a);
+                CKL();
+                acc_dirty = true;
+                break;
+            case MPS_PHASE_MKPRS:
+                need_lists();
+                if (diag_on) k_ph_prs<R, RN, true><<<gb, block, 0, stream>>>(a);
+                else k_ph_prs<R, RN, false><<<gb, block, 0, stream>>>(a);
+                CKL();
+                break;
+            case MPS_PHASE_PRSGRDTRM:
+                need_lists();
+                if (diag_on) k_ph_grd<R, RN, true><<<gb, block, 0, stream>>>(a);
+                else k_ph_grd<R, RN, false><<<gb, block, 0, stream>>>(a);
+                CKL();
+                acc_dirty = true;
+                break;
+            case MPS_PHASE_UPPCL2:
+                k_ph_uppcl2<R, RN><<<gb, block, 0, stream>>>(a);
+                CKL();
+                sorted = false;
+                acc_dirty = true;
+                break;
+            default:
+                throw ApiError(MPS_ERR_ARG, "unknown phase " + std::to_string(ph));
+        }
+    }
+
+    // ---- state I/O ---------------------------------------------------------------------
+    void load_fluid(bool use_acc) {
+        k_load_fluid<R><<<blocks(nF, 256), 256, 0, stream>>>(io, d_fluid_ids, nF, S.pos, S.vel,
+                                                             S.acc, S.prs, S.pav, S.pid, S.typ,
+                                                             use_acc ? 1 : 0);
+        CKL();
+        lists_valid = sorted = m1_valid = false;
+        acc_dirty = use_acc;
+    }
+
+    void store_all() {
+        k_store_fluid<R, RN><<<blocks(nF, 256), 256, 0, stream>>>(io, d_sc, nscene, nF, S.pos, S.vel,
+                                                                  S.acc, S.prs, S.pav, S.pid, S.typ);
+        CKL();
+        if (nW > 0) {
+            k_store_walls<R, RN><<<blocks(nW, 256), 256, 0, stream>>>(io, d_sc, nscene, nW, w_pos,
+                                                                      w_vel, w_id, w_typ);
+            CKL();
+        }
+    }
+
+    void get_state(int8_t* typ, void* pos, void* vel, void* acc, void* prs, void* pav) override {
+        store_all();
+        const size_t n3 = 3 * size_t(nT) * sizeof(R), n1 = size_t(nT) * sizeof(R);
+        if (typ) CK(cudaMemcpyAsync(typ, io.typ, nT, cudaMemcpyDeviceToHost, stream));
+        if (pos) CK(cudaMemcpyAsync(pos, io.pos, n3, cudaMemcpyDeviceToHost, stream));
+        if (vel) CK(cudaMemcpyAsync(vel, io.vel, n3, cudaMemcpyDeviceToHost, stream));
+        if (acc) CK(cudaMemcpyAsync(acc, io.acc, n3, cudaMemcpyDeviceToHost, stream));
+        if (prs) CK(cudaMemcpyAsync(prs, io.prs, n1, cudaMemcpyDeviceToHost, stream));
+        if (pav) CK(cudaMemcpyAsync(pav, io.pav, n1, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    void set_state(const int8_t* typ, const void* pos, const void* vel, const void* acc,
+                   const void* prs, const void* pav) override {
+        // start from the current state so that omitted arrays keep their values
+        store_all();
+        const size_t n3 = 3 * size_t(nT) * sizeof(R), n1 = size_t(nT) * sizeof(R);
+        if (typ) CK(cudaMemcpyAsync(io.typ, typ, nT, cudaMemcpyHostToDevice, stream));
+        if (pos) CK(cudaMemcpyAsync(io.pos, pos, n3, cudaMemcpyHostToDevice, stream));
+        if (vel) CK(cudaMemcpyAsync(io.vel, vel, n3, cudaMemcpyHostToDevice, stream));
+        if (acc) CK(cudaMemcpyAsync(io.acc, acc, n3, cudaMemcpyHostToDevice, stream));
+        if (prs) CK(cudaMemcpyAsync(io.prs, prs, n1, cudaMemcpyHostToDevice, stream));
+        if (pav) CK(cudaMemcpyAsync(io.pav, pav, n1, cudaMemcpyHostToDevice, stream));
+        load_fluid(true);
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    void get_wall_flags(int8_t* out) override {
+        std::vector<int8_t> se(std::max(nW, 1));
+        if (nW > 0) {
+            CK(cudaMemcpyAsync(se.data(), w_se, nW, cudaMemcpyDeviceToHost, stream));
+            std::vector<int> ids(nW);
+            CK(cudaMemcpyAsync(ids.data(), w_id, sizeof(int) * nW, cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            std::memset(out, 0, nT);
+            for (int w = 0; w < nW; ++w) out[ids[w]] = se[w];
+        } else {
+            std::memset(out, 0, nT);
+        }
+    }
+
+    int get_mirrors(int which, int cp, int32_t* slot, void* pos, void* prs) override {
+        int n = 0;
+        const MirrorBuf<R>* b = which == 2 ? &M2 : (which == 1 ? &M1 : &U);
+        if (which == 0) {
+            CK(cudaMemcpyAsync(&n, &cnt->mirror_raw, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        } else {
+            CK(cudaMemcpyAsync(&n, (which == 2 ? mcs2 : mcs1) + dead(), sizeof(int),
+                               cudaMemcpyDeviceToHost, stream));
+        }
+        CK(cudaStreamSynchronize(stream));
+        n = std::min(n, cap);
+        std::vector<V4<R>> p(std::max(n, 1));
+        std::vector<int> s(std::max(n, 1));
+        if (n > 0) {
+            CK(cudaMemcpyAsync(p.data(), b->pos, sizeof(V4<R>) * n, cudaMemcpyDeviceToHost, stream));
+            CK(cudaMemcpyAsync(s.data(), b->slot, sizeof(int) * n, cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+        }
+        std::vector<int> order;
+        for (int k = 0; k < n; ++k)
+            if (s[k] >= 0) order.push_back(k);
+        std::sort(order.begin(), order.end(), [&](int a, int b2) { return s[a] < s[b2]; });
+        int m = int(order.size());
+        for (int k = 0; k < m && k < cp; ++k) {
+            int q = order[k];
+            if (slot) slot[k] = s[q];
+            if (pos) {
+                R* o = static_cast<R*>(pos);
+                o[k] = p[q].x; o[cp + k] = p[q].y; o[2 * size_t(cp) + k] = p[q].z;
+            }
+            if (prs) static_cast<R*>(prs)[k] = p[q].w;
+        }
+        return m;
+    }
+
+    void get_diag(int32_t* table, void* nd) override {
+        store_all();  // refreshes io.cell from the current positions
+        std::vector<int> cell(nT);
+        CK(cudaMemcpyAsync(cell.data(), io.cell, sizeof(int) * nT, cudaMemcpyDeviceToHost, stream));
+        if (table)
+            CK(cudaMemcpyAsync(table, diag, sizeof(int32_t) * kDiagCols * size_t(nT),
+                               cudaMemcpyDeviceToHost, stream));
+        std::vector<RN> ndn(nT);
+        CK(cudaMemcpyAsync(ndn.data(), ndens, sizeof(RN) * nT, cudaMemcpyDeviceToHost, stream));
+        std::vector<int8_t> ty(nT);
+        CK(cudaMemcpyAsync(ty.data(), io.typ, nT, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        if (table)
+            for (int i = 0; i < nT; ++i) table[size_t(i) * kDiagCols] = ty[i] == kGST ? -1 : cell[i];
+        if (nd)
+            for (int i = 0; i < nT; ++i) static_cast<R*>(nd)[i] = R(ndn[i]);
+    }
+
+    void get_counters(mps_counters* o) override {
+        DevCounters c;
+        int a1 = 0, a2 = 0, alive = 0;
+        CK(cudaMemcpyAsync(&c, cnt, sizeof(c), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(&a1, mcs1 + dead(), sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(&a2, mcs2 + dead(), sizeof(int), cudaMemcpyDeviceToHost, stream));
+        std::vector<int8_t> ty(std::max(nF, 1));
+        CK(cudaMemcpyAsync(ty.data(), S.typ, std::max(nF, 1), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        for (int k = 0; k < nF; ++k) alive += ty[k] == kFLD;
+        std::memset(o, 0, sizeof(*o));
+        o->steps = steps;
+        o->n_fluid_alive = alive;
+        o->n_deleted = nF - alive;
+        o->n_mirror_1 = a1;
+        o->n_mirror_2 = a2;
+        o->err_mirror_slot = c.err_mirror_slot;
+        o->err_mirror_capacity = c.err_capacity;
+        o->err_cell_range = c.err_cell;
+        o->err_nan = c.err_nan;
+    }
+
+    void integrals(int scene, double out[6]) override {
+        if (!lists_valid) mkbkt(acc_dirty);
+        std::vector<double> init(6 * size_t(nscene), 0.0);
+        for (int s = 0; s < nscene; ++s) init[6 * s + 4] = -1e300;
+        CK(cudaMemcpyAsync(d_integ, init.data(), sizeof(double) * init.size(), cudaMemcpyHostToDevice,
+                           stream));
+        dim3 grid(std::min(blocks(std::max(nF, 1), 256), 148 * 4), nscene);
+        k_integrals<R, RN><<<grid, 256, 0, stream>>>(d_sc, cs, S.pos, S.vel, S.typ, d_nbxyz, d_integ);
+        CKL();
+        CK(cudaMemcpyAsync(init.data(), d_integ, sizeof(double) * init.size(), cudaMemcpyDeviceToHost,
+                           stream));
+        CK(cudaStreamSynchronize(stream));
+        const double* v = init.data() + 6 * scene;
+        double n = v[5];
+        out[0] = n > 0 ? v[0] / n : 0;
+        out[1] = n > 0 ? v[1] / n : 0;
+        out[2] = n > 0 ? v[2] / n : 0;
+        out[3] = v[3];
+        out[4] = n > 0 ? v[4] : 0;
+        out[5] = n;
+    }
+};
+
+// one explicit instantiation per translation unit (mps_inst_*.cu)
+SolverBase* make_solver_f32(int ns, const mps_params* p, const int32_t* c, const int8_t* t,
+                            const void* pos, const void* vel, const void* nrm);
+SolverBase* make_solver_f64(int ns, const mps_params* p, const int32_t* c, const int8_t* t,
+                            const void* pos, const void* vel, const void* nrm);
+SolverBase* make_solver_mix(int ns, const mps_params* p, const int32_t* c, const int8_t* t,
+                            const void* pos, const void* vel, const void* nrm);
+
+}  // namespace mps

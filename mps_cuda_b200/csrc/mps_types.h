@@ -1,0 +1,66 @@
+// mps_types.h -- host/device data layout of the B200 MPS solver.
+//
+// Particle state lives in HBM as arrays of 4-wide vectors (16 B per float particle,
+// 32 B per double particle) sorted by bucket: bucket-major in the reference's bucket
+// order ib = iz*nBxy + iy*nBx + ix (kernel.cu:521-524), ascending particle id inside a
+// bucket. Walls are static and kept in their own sorted arrays; mirrors are a compact
+// list sorted by (bucket, slot id) instead of the reference's NumMRR slots per particle
+// (kernel.cu:96-103).
+#pragma once
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define MPS_HD __host__ __device__ __forceinline__
+#else
+#define MPS_HD inline
+#endif
+
+namespace mps {
+
+constexpr int kGST = -1, kFLD = 0, kWLL = 1, kOBJ = 2, kOBJ2 = 3, kMRR = 4;
+constexpr int kEDGE = 1;
+constexpr int kNumMRR = 10;  // const.cuh:50
+
+template <class R> struct alignas(4 * sizeof(R)) V4 {
+    R x, y, z, w;
+};
+
+// Per-scene constants, derived on the host exactly as AlcBkt/SetPara do (kernel.cu:307-415).
+template <class R, class RN> struct SceneDev {
+    R minc[3];        // padded domain minimum (kernel.cu:26-28)
+    R dbinv, db;      // bucket width 3.1 l0 and its inverse (kernel.cu:313-315)
+    int nbx, nby, nbz, nbxy;
+    int cbase;        // first global bucket of this scene
+    int pbase;        // first global particle id of this scene
+    int pcount;       // particles of this scene
+    int pad0;
+    R r, r2, r_le;    // Laplacian radius; r_le = largest t with sqrt(t) <= r
+    R rp, rp2, rp_lt; // gradient radius; rp_lt = largest t with sqrt(t) < rp
+    R rlim2, rlimw2;  // collision radii (kernel.cu:370-371, 1184-1185)
+    R list_thr;       // d2 bound of the neighbour lists shared by ChkCol/MkPrs/PrsGrdTrm
+    R edge_r2;        // Surface_Edge radius^2 (kernel.cu:558)
+    R wall_dist0;     // 10 r (kernel.cu:940)
+    R two_l0, kn;     // 2 l0; KNM_VSC / n0 (kernel.cu:1113)
+    R g[3];
+    R dt, umax;
+    R lo[3], hi[3];   // ChkPcl box (kernel.cu:484-486)
+    R colfac;         // COL * mj / (mi + mj) (kernel.cu:1215)
+    R invro, a3;      // -1/rho, 3/n0_grad (kernel.cu:1659, 1665)
+    // (radius + margin)^2 used to skip bucket rows: r, rp, rlim, 0.45 l0, max(rlim, rp)
+    R skip_r, skip_rp, skip_rl, skip_rw, skip_rc;
+    RN n0g, prs_coef, pmax, rho;          // number density / EOS in RN (kernel.cu:1388-1406)
+    RN rp_n;
+};
+
+struct DevCounters {
+    int mirror_raw;       // entries appended to the raw mirror list
+    int err_mirror_slot;  // corner mirror without a free slot (kernel.cu:868-874)
+    int err_capacity;     // raw mirror list full
+    int err_cell;         // bucket index clamped into the grid
+    int err_nan;          // non-finite position met in a bucket build
+    int n_m1, n_m2;       // alive mirrors after the latest generations
+    int deleted;          // particles deleted by ChkPcl (cumulative)
+    int pad[8];
+};
+
+}  // namespace mps

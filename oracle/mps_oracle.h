@@ -1,0 +1,58 @@
+/*
+ * mps_oracle.h -- C-ABI of the CPU oracle (TEST INFRASTRUCTURE, not the product).
+ *
+ * The oracle is a CPU restatement of the explicit MPS step of frsykzk/MPS_CUDA
+ * (kernel.cu:307-1944), OpenMP over particles, templated on the arithmetic type. It keeps
+ * the reference's data layout (arrays in particle-id order, NumMRR mirror slots per
+ * particle) and runs the reference's per-particle loop bodies. It is used only by the
+ * tests, by the `cpu_baseline` leg of bench.py and by bench.py's reference arm; the
+ * product (mps_cuda_b200) never links or calls it.
+ *
+ * The parameter struct has the same field order as mps_params in include/mps_b200.h so
+ * that callers can fill both from one record.
+ */
+#ifndef MPS_ORACLE_H
+#define MPS_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_params {
+    double pcl_dst, min[3], max[3], g[3], knm_vsc, col_rat, dst_lmt_rat, rho, snd, dt, umax,
+        pmax;
+    int32_t precision; /* 0 float, 1 double, 2 float state + double number density */
+    int32_t reserved[7];
+} oracle_params;
+
+void* oracle_create(const oracle_params* p, int32_t n, const int8_t* typ, const void* pos,
+                    const void* vel, const void* nrm);
+void oracle_destroy(void* h);
+int oracle_set_threads(int32_t n);
+/* phase numbering is MPS_PHASE_* of include/mps_b200.h */
+int oracle_phase(void* h, int32_t phase);
+int oracle_step(void* h, int32_t nsteps);
+int oracle_get_state(void* h, int8_t* typ, void* pos, void* vel, void* acc, void* prs,
+                     void* pav);
+int oracle_set_state(void* h, const int8_t* typ, const void* pos, const void* vel,
+                     const void* acc, const void* prs, const void* pav);
+int oracle_get_wall_flags(void* h, int8_t* wllse);
+int oracle_set_wall_flags(void* h, const int8_t* wllse);
+/* MRR slots in ascending slot order; pos is SoA with stride cap */
+int oracle_get_mirrors(void* h, int32_t cap, int32_t* slot, void* pos, void* prs,
+                       int32_t* n_out);
+/* replace every mirror slot: slots not listed become GST */
+int oracle_set_mirrors(void* h, int32_t n, const int32_t* slot, const void* pos,
+                       const void* prs);
+/* [n][11] table, columns MPS_DIAG_*; ndens[n] (real) */
+int oracle_get_diag(void* h, int32_t* table, void* ndens);
+/* out[0..]: n0, lmd, n0_grad, lmd_grad, numn0_grad, r, rp, db, dbinv, nbx, nby, nbz,
+ * rlim2, col, prs_coef, minc xyz, maxc xyz */
+int oracle_get_info(void* h, double* out);
+/* out[6]: centroid xyz, sum |v|^2/2, max x, alive count (fluid) */
+int oracle_get_integrals(void* h, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

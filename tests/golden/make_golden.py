@@ -1,0 +1,80 @@
+"""Generate the golden vectors of the reference's own kernels (run on a machine with a GPU).
+
+Runs frsykzk/MPS_CUDA's `class MPS` (built by oracle/ref_build.sh, driven through
+oracle/ref_harness.cu) on a small seeded dam break and records the state after every method
+call of two time steps of ClcMPS's loop body (kernel.cu:1904-1935): the fluid particles'
+type, position, velocity, acceleration, pressure and averaged pressure, the live mirror
+particles (slot, position, pressure), and the bucket of every particle read back from the
+reference's linked lists. The CPU tests replay each method of the oracle from the recorded
+input state and compare with the recorded output state.
+
+    python tests/golden/make_golden.py [outdir]
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from mps_cuda_b200.solver import SceneDesc, dambreak, dambreak_params  # noqa: E402
+from oracle import refbind  # noqa: E402
+
+SCENE = SceneDesc(0.02, (0.24, 0.12, 0.24), (6, 4, 8), seed=3)
+DT = 2e-4
+RECORD_STEPS = (0, 3)
+FIELDS = ("typ", "pos", "vel", "acc", "prs", "pav")
+
+
+def params_array(p) -> np.ndarray:
+    return np.array([p.pcl_dst, *p.min, *p.max, *p.g, p.knm_vsc, p.col_rat, p.dst_lmt_rat, p.rho,
+                     p.snd, p.dt, p.umax, p.pmax, p.precision], np.float64)
+
+
+def snapshot(ref, nf, tag, out):
+    st = ref.state()
+    for k in FIELDS:
+        a = st[k]
+        out[f"{tag}_{k}"] = a[..., :nf].copy()
+    m = ref.mirrors()
+    out[f"{tag}_mslot"] = m["slot"]
+    out[f"{tag}_mpos"] = m["pos"]
+    out[f"{tag}_mprs"] = m["prs"]
+    out[f"{tag}_cell"] = ref.buckets()
+
+
+def main(outdir: str):
+    os.makedirs(outdir, exist_ok=True)
+    for prec, name in ((0, "f32"), (1, "f64")):
+        dty = np.float64 if prec == 1 else np.float32
+        sc = dambreak(SCENE)
+        p = dambreak_params(SCENE, dt=DT, precision=prec)
+        args = (sc["typ"], sc["pos"].astype(dty), sc["vel"].astype(dty), sc["nrm"].astype(dty))
+        ref = refbind.Reference(p, *args)
+        nf = int(np.sum(sc["typ"] == 0))
+        assert np.all(sc["typ"][:nf] == 0) and np.all(sc["typ"][nf:] != 0)
+        out = {"params": params_array(p), "typ": sc["typ"], "pos": args[1], "vel": args[2],
+               "nrm": args[3], "nf": np.array(nf), "wllse": ref.wall_flags(),
+               "phases": np.array(refbind.STEP_PHASES, np.int32),
+               "record_steps": np.array(RECORD_STEPS, np.int32)}
+        info = ref.info()
+        out["ref_info"] = np.array([info[k] for k in sorted(info)], np.float64)
+        out["ref_info_keys"] = np.array(sorted(info))
+        for step in range(max(RECORD_STEPS) + 1):
+            rec = step in RECORD_STEPS
+            if rec:
+                snapshot(ref, nf, f"s{step}_k0", out)
+            for k, ph in enumerate(refbind.STEP_PHASES):
+                ref.phase(ph)
+                if rec:
+                    snapshot(ref, nf, f"s{step}_k{k + 1}", out)
+        path = os.path.join(outdir, f"ref_small_{name}.npz")
+        np.savez_compressed(path, **out)
+        print(path, os.path.getsize(path))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden"))

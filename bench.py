@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Throughput of the explicit MPS step on B200: particle-updates/s.
+
+A step is one pass of the dam-break time step (frsykzk/MPS_CUDA kernel.cu:1904-1941) over
+all fluid particles of the workload; a particle-update is one fluid particle advanced
+through one step. The default workload is the 384 000-particle dam break (l0 = 0.005 m,
+0.4 x 0.2 x 0.6 m column in a 1.6 x 0.2 x 0.8 m tank, dt = 5e-5 s), FP32, on synthetic
+seeded inputs (there is no dataset).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours      : libmps_b200.so. `value` = device time of K steps (CUDA events on the solver's
+            stream, L2 flushed between steps, max over ranks); `e2e` = the same steps
+            through the C-ABI with the state uploaded from and read back into pinned host
+            buffers every step; `roofline` = the dominant kernel group's algorithmic bytes
+            per launch over its average launch time, timed live with CUDA events;
+            `cpu_baseline` = the CPU oracle (OpenMP restatement of the reference's
+            per-particle loops) on a bounded sample of the same workload, rank 0 only.
+reference : the reference's per-particle loops as that OpenMP CPU restatement (the
+            reference itself has no CPU implementation), all host threads, rank 0 only.
+Under torchrun (N > 1) each rank advances its own copy of the workload on its own GPU
+(replicas: the step has no exchange between scenes), so `value` counts all ranks' updates.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-updates/s"
+WORKLOAD = "dambreak_l0.005_384k"
+L2_FLUSH_BYTES = 512 << 20  # > 126 MB L2
+
+# Algorithmic bytes per unit (s = sizeof(real)): the state each kernel group must move,
+# neighbour re-reads counted as cache hits.
+#   pass A  (VscTrm + UpPcl1)  : read x, v; write x*, v*             12 s / fluid particle
+#                                + read M1 mirrors                    3 s / mirror
+#   pass B  (ChkCol + MkPrs)   : read x*, v*; write v**, P           10 s / fluid particle
+#                                + read M1 mirrors                    3 s / mirror
+#   pass C  (PrsGrdTrm+UpPcl2) : read x*, v**, P, pav; write x, v, pav 15 s / fluid particle
+#                                + read M2 mirrors (x, P)              4 s / mirror
+#   gen     (GenMRR + MRRinout): read x, P; write mirrors (x, P, slot) 4 s / fluid particle
+#                                                                   + (4 s + 4) / mirror
+#   bin     (bucket build)     : read key state, write sorted state  2 x payload / item
+
+
+def alg_bytes(group: str, s: int, nf: int, m1: int, m2: int) -> float:
+    return {
+        "pass_a": 12 * s * nf + 3 * s * m1,
+        "pass_b": 10 * s * nf + 3 * s * m1,
+        "pass_c": 15 * s * nf + 4 * s * m2,
+        "gen_cull": 4 * s * nf + (4 * s + 4) * (m1 + m2) / 2,
+        "bin_fluid": 2 * (8 * s + 13) * nf,
+        "bin_mirror": 2 * (4 * s + 4) * (m1 + m2) / 2,
+    }[group]
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dram_traffic(workload: str, precision: str):
+    """Per-launch DRAM bytes of each kernel group from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if not os.path.exists(p):
+        return {}
+    d = json.load(open(p))
+    return d.get(f"{workload}:{precision}", {})
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def setup_dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl" if os.environ.get("MPS_BENCH_BACKEND") != "gloo" else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def allreduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def build_scene(workload: str, precision: str):
+    from mps_cuda_b200 import F32, F32_N64, F64, configs, dambreak, dambreak_params
+    desc, dt, _ = configs.WORKLOADS[workload]
+    prec = {"f32": F32, "f64": F64, "f32n64": F32_N64}[precision]
+    sc = dambreak(desc)
+    p = dambreak_params(desc, dt=dt, precision=prec)
+    rd = np.float64 if prec == F64 else np.float32
+    return p, sc["typ"], sc["pos"].astype(rd), sc["vel"].astype(rd), sc["nrm"].astype(rd)
+
+
+def cpu_oracle_rate(p, typ, pos, vel, nrm, budget_s: float, max_steps: int, warmup: int = 1):
+    """Particle-updates/s of the OpenMP oracle; returns (rate, steps timed, threads)."""
+    from oracle.oracle import Oracle, lib, params_from
+    threads = os.cpu_count() or 1
+    lib().oracle_set_threads(threads)
+    o = Oracle(params_from(p), typ, pos, vel, nrm)
+    nf = int((typ == 0).sum())
+    t0 = time.perf_counter()
+    o.step(max(warmup, 1))
+    t_step = (time.perf_counter() - t0) / max(warmup, 1)
+    k = int(max(1, min(max_steps, budget_s // max(t_step, 1e-9))))
+    t0 = time.perf_counter()
+    o.step(k)
+    el = time.perf_counter() - t0
+    o.close()
+    return nf * k / el, k, threads, el
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    p, typ, pos, vel, nrm = build_scene(args.workload, args.precision)
+    rate, k, threads, el = cpu_oracle_rate(p, typ, pos, vel, nrm, budget_s=150.0,
+                                           max_steps=args.steps, warmup=min(args.warmup, 2))
+    sample = (f"{k} full steps of the {args.workload} workload ({int((typ == 0).sum())} fluid "
+              f"particles) after {min(args.warmup, 2)} warm-up step(s), {threads} OpenMP threads")
+    line = {"metric": METRIC, "value": rate, "unit": "particle-updates/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": k, "warmup": min(args.warmup, 2),
+            "ms_per_step": 1e3 * el / k, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+            "config": {"workload": args.workload, "precision": args.precision,
+                       "implementation": "OpenMP CPU restatement of the reference's per-particle "
+                                         "loops (the reference has no CPU path)"},
+            "cpu_baseline": {"value": rate, "unit": "particle-updates/s", "cores": threads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": rate, "unit": "particle-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from mps_cuda_b200 import MPS, select_device
+    from mps_cuda_b200 import _lib as L
+
+    torch.cuda.set_device(local)
+    select_device(local)
+    p, typ, pos, vel, nrm = build_scene(args.workload, args.precision)
+    nf = int((typ == 0).sum())
+    s = 8 if args.precision == "f64" else 4
+    g = MPS(p, typ, pos, vel, nrm)
+    stream = torch.cuda.Stream()
+    g.set_stream(stream.cuda_stream)
+    g.set_option(L.OPT_GRAPH, 1)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    # warm-up (also captures the step graph)
+    for _ in range(max(args.warmup, 3)):
+        g.step(1)
+    g.synchronize()
+
+    # ---- timed region: K steps, L2 flushed between steps (outside the events) ----------
+    K = args.steps
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    l0 = g.counters()["kernel_launches"]
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = ClockSampler(local).__enter__()  # sampled through every measured loop below
+    w0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            flush.fill_(float(k))
+            e0[k].record(stream)
+            g.step(1)
+            e1[k].record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    barrier(world)
+    launches = g.counters()["kernel_launches"] - l0
+    dev_ms = sum(a.elapsed_time(b) for a, b in zip(e0, e1))
+    dev_ms_max = allreduce_max(dev_ms, world)
+    value = world * nf * K / (dev_ms_max / 1e3)
+    cnt = g.counters()
+
+    # ---- per-kernel device times (CUDA events on the solver's stream), same workload ---
+    g.set_option(L.OPT_TIMING, 1)
+    g.timing(reset=True)
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            flush.fill_(float(k))
+            g.step(1)
+    tm = g.timing(reset=True)
+    g.set_option(L.OPT_TIMING, 0)
+    m1, m2 = cnt["n_mirror_1"], cnt["n_mirror_2"]
+    groups = {}
+    for name, (ms, n) in tm.items():
+        if n:
+            groups[name] = {"ms_per_launch": ms / n, "launches": n, "share": 0.0,
+                            "alg_bytes": alg_bytes(name, s, nf, m1, m2)}
+    total = sum(v["ms_per_launch"] * v["launches"] for v in groups.values())
+    for v in groups.values():
+        v["share"] = v["ms_per_launch"] * v["launches"] / total
+    dom = max(groups, key=lambda k_: groups[k_]["ms_per_launch"] * groups[k_]["launches"])
+    peak, peak_kind = peaks()
+    ach = groups[dom]["alg_bytes"] / (groups[dom]["ms_per_launch"] / 1e3) / 1e9
+    traffic = dram_traffic(args.workload, args.precision).get(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak, "traffic": traffic, "peak_source": peak_kind,
+                "alg_bytes_per_launch": groups[dom]["alg_bytes"],
+                "ms_per_launch": groups[dom]["ms_per_launch"]}
+
+    # ---- end to end through the C-ABI with pinned host buffers --------------------------
+    e2e = None
+    if not args.no_e2e:
+        st0 = g.state()
+        pinned = {k: torch.empty(v.shape, dtype=torch.from_numpy(v[:1].copy()).dtype,
+                                 pin_memory=True).numpy() for k, v in st0.items()}
+        for k, v in st0.items():
+            pinned[k][...] = v
+        out = {k: torch.empty(v.shape, dtype=torch.from_numpy(v[:1].copy()).dtype,
+                              pin_memory=True).numpy() for k, v in st0.items()}
+        h2d = sum(v.nbytes for v in pinned.values())
+        d2h = sum(v.nbytes for v in out.values())
+        g.set_stream(0)
+        barrier(world)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        for k in range(K):
+            g.set_state(**pinned)  # this step's input from pinned host memory
+            g.step(1)
+            g.state(out=out)       # and its result back
+            pinned, out = out, pinned
+        el = time.perf_counter() - w0
+        el = allreduce_max(el, world)
+        e2e = {"value": world * nf * K / el, "unit": "particle-updates/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": 1e3 * el / K}
+
+    clk.__exit__(None, None, None)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, k, threads, el = cpu_oracle_rate(p, typ, pos, vel, nrm, budget_s=20.0, max_steps=10)
+        cpu = {"value": rate, "unit": "particle-updates/s", "cores": threads, "kind": "port",
+               "sample": f"{k} steps of the same workload after 1 warm-up step ({el:.1f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-updates/s", "n_gpus": world,
+            "steps": K, "warmup": max(args.warmup, 3), "ms_per_step": dev_ms_max / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": args.precision, "data": "synthetic",
+            "config": {"workload": args.workload, "fluid_particles": nf,
+                       "wall_particles": int((typ != 0).sum()), "precision": args.precision,
+                       "l2": "flushed between timed steps (512 MiB write)",
+                       "parallelism": f"replicas x{world}", "graph": True},
+            "clocks": clk.summary(), "wall_ms_per_step": 1e3 * wall / K,
+            "e2e": e2e, "gpu_launches": launches,
+            "roofline": roofline, "kernel_groups": groups, "cpu_baseline": cpu,
+            "counters": {k: v for k, v in cnt.items() if k != "kernel_launches"},
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--precision", choices=["f32", "f64", "f32n64"], default="f32")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = setup_dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -106,7 +106,9 @@ typedef struct mps_counters {
     int32_t err_mirror_capacity;   /* mirror buffer full                                    */
     int32_t err_cell_range;        /* a bucket index left the grid and was clamped          */
     int32_t err_nan;               /* non-finite position met in a bucket build             */
-    int32_t reserved[6];
+    int32_t reserved0;
+    int64_t kernel_launches;       /* kernels this handle launched (graph replays included) */
+    int32_t reserved[2];
 } mps_counters;
 
 /* Per-particle diagnostic counters (mps_get_diag), column order of the int32 table. */
@@ -146,7 +148,20 @@ enum {
     MPS_OPT_DIAG = 0,        /* 1: record per-particle neighbour counts (slower)        */
     MPS_OPT_GRAPH = 1,       /* 1: replay mps_step through a captured CUDA graph        */
     MPS_OPT_BLOCK = 2,       /* threads per block of the neighbour passes (0 = tuned)   */
-    MPS_OPT_CELL_SKIP = 3    /* 1: skip bucket rows outside the radius (default 1)      */
+    MPS_OPT_CELL_SKIP = 3,   /* 1: skip bucket rows outside the radius (default 1)      */
+    MPS_OPT_TIMING = 4       /* 1: time every kernel group of mps_step with CUDA events
+                                on the handle's stream (steps then run without a graph) */
+};
+
+/* Kernel groups reported by mps_get_timing. */
+enum {
+    MPS_K_PASS_A = 0,       /* VscTrm + UpPcl1                                   */
+    MPS_K_PASS_B = 1,       /* ChkCol + MkPrs                                    */
+    MPS_K_PASS_C = 2,       /* PrsGrdTrm + UpPcl2                                */
+    MPS_K_GEN = 3,          /* GenMRR_nonslip + MRRinout (both generations)      */
+    MPS_K_BIN_FLUID = 4,    /* fluid bucket builds (MkBkt)                       */
+    MPS_K_BIN_MIRROR = 5,   /* mirror bucket builds (MkBkt_MRR)                  */
+    MPS_K_COUNT = 6
 };
 
 typedef struct mps_handle mps_handle;
@@ -181,7 +196,18 @@ int mps_scene_dambreak(const mps_scene_desc* d, int32_t cap, int8_t* typ, double
 int mps_params_dambreak(const mps_scene_desc* d, double snd, double dt, double knm_vsc,
                         double g_z, int32_t precision, mps_params* p);
 
+/*
+ * Derived constants of one scene without creating a solver (host only, no GPU needed):
+ * the values AlcBkt and SetPara compute (kernel.cu:307-373). n_particles/n_fluid/n_wall
+ * are left zero.
+ */
+int mps_derive(const mps_params* p, mps_info* out);
+
 /* ---- handle life cycle ------------------------------------------------------------ */
+
+/* Make `device` current for the calling host thread; handles created afterwards on this
+ * thread live on it (one process per GPU: call once per rank before mps_create). */
+int mps_select_device(int32_t device);
 
 /*
  * Create a solver for one scene. Replaces RdDat + AlcBkt + SetPara (kernel.cu:4-143,
@@ -227,16 +253,24 @@ int mps_set_state(mps_handle* h, const int8_t* typ, const void* pos, const void*
 /* WLLSE flags of every particle (Surface for non-walls), kernel.cu:553-668. */
 int mps_get_wall_flags(mps_handle* h, int8_t* wllse);
 /*
- * Mirrors of the latest generation (`which` = 1: the set the viscosity / collision /
- * density steps read, 2: the set the pressure gradient reads), sorted by slot id
- * = i*MPS_NUM_MRR + k as in the reference's d_TypM layout (kernel.cu:689-893).
- * pos is SoA with stride `cap`. *n_out receives the count even if it exceeds cap.
+ * Mirror particles, sorted by slot id = i*MPS_NUM_MRR + k as in the reference's d_TypM
+ * layout (kernel.cu:689-893). `which` = 2: the second generation of the last step (what the
+ * reference's mirror arrays hold after a step: GenMRR at x*, read by PrsGrdTrm);
+ * 1: the first generation (read by VscTrm, ChkCol, MkPrs). After mps_step, set 1 already
+ * holds the next step's first generation, made from the new positions; after the
+ * MPS_PHASE_* calls it is the set MkBkt_MRR produced last. 0: the raw (unculled) output of
+ * the last GenMRR_nonslip phase. pos is SoA with stride `cap`; *n_out receives the count
+ * even if it exceeds cap.
  */
 int mps_get_mirrors(mps_handle* h, int32_t which, int32_t cap, int32_t* slot, void* pos,
                     void* prs, int32_t* n_out);
 /* Per-particle diagnostic table [n_particles][MPS_DIAG_NCOL] and number density n_i. */
 int mps_get_diag(mps_handle* h, int32_t* table, void* ndens);
 int mps_get_counters(mps_handle* h, mps_counters* out);
+/* Accumulated device time (ms) and launch count of kernel group `kernel` (MPS_K_*) over the
+ * steps run with MPS_OPT_TIMING on; `reset` != 0 clears the accumulators afterwards. */
+int mps_get_timing(mps_handle* h, int32_t kernel, double* total_ms, int64_t* launches,
+                   int32_t reset);
 /*
  * Integrals of scene `scene`: out[0..2] fluid centroid, out[3] kinetic energy per unit
  * mass (sum |v|^2 / 2), out[4] surge front (max x of fluid), out[5] alive fluid count.

@@ -6,8 +6,9 @@ The solver itself is ``libmps_b200.so`` (hand-written sm_100a kernels behind the
 """
 from ._lib import (F32, F32_N64, F64, FLD, GST, MRR, OBJ, OBJ2, WLL, MPSError, lib,
                    library_path)
-from .solver import MPS, MPSBatch, SceneDesc, dambreak, dambreak_params, real_dtype
+from .solver import (MPS, MPSBatch, SceneDesc, dambreak, dambreak_params, derive, real_dtype,
+                     select_device)
 
-__all__ = ["MPS", "MPSBatch", "SceneDesc", "dambreak", "dambreak_params", "MPSError", "lib",
+__all__ = ["MPS", "MPSBatch", "SceneDesc", "dambreak", "dambreak_params", "derive", "select_device", "MPSError", "lib",
            "library_path", "real_dtype", "F32", "F64", "F32_N64", "GST", "FLD", "WLL", "OBJ",
            "OBJ2", "MRR"]

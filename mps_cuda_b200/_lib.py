@@ -28,7 +28,8 @@ NUM_MRR = 10
 F32, F64, F32_N64 = 0, 1, 2
 (PHASE_MKBKT, PHASE_SURFACE_EDGE, PHASE_RESETMRR, PHASE_GENMRR_NONSLIP, PHASE_MKBKT_MRR,
  PHASE_VSCTRM, PHASE_UPPCL1, PHASE_CHKCOL, PHASE_MKPRS, PHASE_PRSGRDTRM, PHASE_UPPCL2) = range(11)
-OPT_DIAG, OPT_GRAPH, OPT_BLOCK, OPT_CELL_SKIP = 0, 1, 2, 3
+OPT_DIAG, OPT_GRAPH, OPT_BLOCK, OPT_CELL_SKIP, OPT_TIMING = 0, 1, 2, 3, 4
+KERNEL_GROUPS = ["pass_a", "pass_b", "pass_c", "gen_cull", "bin_fluid", "bin_mirror"]
 DIAG_COLUMNS = ["cell", "vsc_f", "vsc_m", "col_f", "col_w", "col_m", "prs_f", "prs_m",
                 "grd_f", "grd_m", "gen_w"]
 
@@ -57,7 +58,8 @@ class mps_counters(C.Structure):
                 ("n_mirror_1", C.c_int32), ("n_mirror_2", C.c_int32),
                 ("err_mirror_slot", C.c_int32), ("err_mirror_capacity", C.c_int32),
                 ("err_cell_range", C.c_int32), ("err_nan", C.c_int32),
-                ("reserved", C.c_int32 * 6)]
+                ("reserved0", C.c_int32), ("kernel_launches", C.c_int64),
+                ("reserved", C.c_int32 * 2)]
 
 
 class mps_scene_desc(C.Structure):
@@ -73,6 +75,8 @@ SIGNATURES = {
                                      c_double_p, c_double_p, c_int32_p]),
     "mps_params_dambreak": (C.c_int, [C.POINTER(mps_scene_desc), C.c_double, C.c_double,
                                       C.c_double, C.c_double, C.c_int32, C.POINTER(mps_params)]),
+    "mps_select_device": (C.c_int, [C.c_int32]),
+    "mps_derive": (C.c_int, [C.POINTER(mps_params), C.POINTER(mps_info)]),
     "mps_create": (C.c_int, [C.POINTER(mps_params), C.c_int32, c_int8_p, C.c_void_p, C.c_void_p,
                              C.c_void_p, C.POINTER(C.c_void_p)]),
     "mps_create_batch": (C.c_int, [C.c_int32, C.POINTER(mps_params), c_int32_p, c_int8_p,
@@ -93,6 +97,8 @@ SIGNATURES = {
                                   C.c_void_p, c_int32_p]),
     "mps_get_diag": (C.c_int, [C.c_void_p, c_int32_p, C.c_void_p]),
     "mps_get_counters": (C.c_int, [C.c_void_p, C.POINTER(mps_counters)]),
+    "mps_get_timing": (C.c_int, [C.c_void_p, C.c_int32, c_double_p, C.POINTER(C.c_int64),
+                                 C.c_int32]),
     "mps_get_integrals": (C.c_int, [C.c_void_p, C.c_int32, c_double_p]),
     "mps_status_string": (C.c_char_p, [C.c_int32]),
     "mps_last_error": (C.c_char_p, []),

@@ -94,6 +94,35 @@ int mps_create_batch(int32_t nscenes, const mps_params* p, const int32_t* counts
     return MPS_OK;
 }
 
+int mps_select_device(int32_t device) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(MPS_ERR_NODEVICE, "no CUDA device");
+    }
+    if (device < 0 || device >= ndev) return fail(MPS_ERR_ARG, "device index out of range");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(MPS_ERR_CUDA, cudaGetErrorString(e));
+    return MPS_OK;
+}
+
+int mps_derive(const mps_params* p, mps_info* out) {
+    if (!p || !out) return fail(MPS_ERR_ARG, "null argument");
+    int rc = check_params(*p);
+    if (rc) return rc;
+    if (p->precision == 1) {
+        mps::SceneDev<double, double> sd;
+        mps::derive_scene<double, double>(*p, 0, 0, 0, sd, *out);
+    } else if (p->precision == 2) {
+        mps::SceneDev<float, double> sd;
+        mps::derive_scene<float, double>(*p, 0, 0, 0, sd, *out);
+    } else {
+        mps::SceneDev<float, float> sd;
+        mps::derive_scene<float, float>(*p, 0, 0, 0, sd, *out);
+    }
+    return MPS_OK;
+}
+
 int mps_create(const mps_params* p, int32_t n, const int8_t* typ, const void* pos,
                const void* vel, const void* nrm, mps_handle** out) {
     return mps_create_batch(1, p, &n, typ, pos, vel, nrm, out);
@@ -130,6 +159,7 @@ int mps_set_option(mps_handle* h, int32_t opt, int32_t value) {
                 s.invalidate_graph();
                 break;
             case MPS_OPT_CELL_SKIP: s.skip_opt = value != 0; s.invalidate_graph(); break;
+            case MPS_OPT_TIMING: s.timing_on = value != 0; break;
             default: throw ApiError(MPS_ERR_ARG, "unknown option");
         }
     });
@@ -189,6 +219,16 @@ int mps_get_diag(mps_handle* h, int32_t* table, void* ndens) {
 int mps_get_counters(mps_handle* h, mps_counters* out) {
     if (!out) return fail(MPS_ERR_ARG, "null buffer");
     return guarded(h, [&](SolverBase& s) { s.get_counters(out); });
+}
+
+int mps_get_timing(mps_handle* h, int32_t kernel, double* total_ms, int64_t* launches,
+                   int32_t reset) {
+    if (kernel < 0 || kernel >= MPS_K_COUNT) return fail(MPS_ERR_ARG, "unknown kernel group");
+    return guarded(h, [&](SolverBase& s) {
+        long long n = 0;
+        s.timing(kernel, total_ms, &n, reset != 0);
+        if (launches) *launches = n;
+    });
 }
 
 int mps_get_integrals(mps_handle* h, int32_t scene, double out[6]) {

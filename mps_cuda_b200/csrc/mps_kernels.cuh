@@ -497,7 +497,7 @@ __global__ void __launch_bounds__(128) k_pass_c(PassArgs<R, RN> a) {
 // of a step (x*, P after pass B) and the first generation of the next one (x^{n+1}, P after
 // pass C). Near-wall particles are a thin layer, so this runs as a light kernel of its own
 // instead of stretching the neighbour passes.
-template <class R, class RN>
+template <class R, class RN, bool DIAG>
 __global__ void __launch_bounds__(128) k_gen_cull(PassArgs<R, RN> a, const V4<R>* gpos,
                                                   const R* gprs, const int8_t* gtyp) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -508,8 +508,9 @@ __global__ void __launch_bounds__(128) k_gen_cull(PassArgs<R, RN> a, const V4<R>
     int ix, iy, iz;
     cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
     RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
-    gen_mirrors<R, RN, true>(sc, c, p.x, p.y, p.z, gprs[s], pid * kNumMRR, a.wl, a.skip != 0,
-                             a.out, a.cnt);
+    int nw = gen_mirrors<R, RN, true>(sc, c, p.x, p.y, p.z, gprs[s], pid * kNumMRR, a.wl,
+                                      a.skip != 0, a.out, a.cnt);
+    if (DIAG) a.diag[size_t(pid) * kDiagCols + DG_GEN_W] = nw;
 }
 
 // ---------------------------------------------------------------------------------------

@@ -39,6 +39,12 @@ struct ApiError : std::runtime_error {
     } while (0)
 
 #define CKL() CK(cudaGetLastError())
+// after a kernel launch inside the solver: count it and check the launch
+#define KL()                          \
+    do {                              \
+        ++launches;                   \
+        CK(cudaGetLastError());       \
+    } while (0)
 
 // ---- derived constants (AlcBkt + SetPara, kernel.cu:307-415) ----------------------------
 template <class R> static R wei(R d, R re) { return ((re / d) + (d / re)) - R(2); }
@@ -201,6 +207,12 @@ struct SolverBase {
     bool diag_on = false, graph_on = false;
     int skip_opt = 1, block = 128;
     long long steps = 0;
+    long long launches = 0;       // kernels launched (graph replays included)
+    long long body_launches = 0;  // kernels of one captured step
+    bool timing_on = false;
+    double t_ms[MPS_K_COUNT] = {};
+    long long t_n[MPS_K_COUNT] = {};
+    virtual void timing(int k, double* ms, long long* n, bool reset) = 0;
     virtual void step(int n) = 0;
     virtual void phase(int ph) = 0;
     virtual void get_state(int8_t*, void*, void*, void*, void*, void*) = 0;
@@ -247,9 +259,70 @@ template <class R, class RN> class Solver final : public SolverBase {
     bool lists_valid = false, sorted = false, m1_valid = false, acc_dirty = false;
     cudaGraphExec_t gexec = nullptr;
     bool gexec_diag = false;
+    // CUDA events bracketing kernel groups when timing_on
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+    cudaEvent_t ev_get() {
+        if (ev_pool.empty()) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            return e;
+        }
+        cudaEvent_t e = ev_pool.back();
+        ev_pool.pop_back();
+        return e;
+    }
+    struct Scope {
+        Solver* s;
+        int k;
+        cudaEvent_t a = nullptr;
+        Scope(Solver* s_, int k_) : s(s_), k(k_) {
+            if (s->timing_on) {
+                a = s->ev_get();
+                CK(cudaEventRecord(a, s->stream));
+            }
+        }
+        ~Scope() {
+            if (!a) return;
+            cudaEvent_t b = nullptr;
+            if (!s->ev_pool.empty()) {
+                b = s->ev_pool.back();
+                s->ev_pool.pop_back();
+            } else if (cudaEventCreate(&b) != cudaSuccess) {
+                b = nullptr;
+            }
+            if (b && cudaEventRecord(b, s->stream) == cudaSuccess) {
+                s->ev_pending.push_back({k, {a, b}});
+            } else {  // timing of this group is lost; the error surfaces at the next check
+                s->ev_pool.push_back(a);
+                if (b) s->ev_pool.push_back(b);
+            }
+        }
+    };
+    void timing(int k, double* ms, long long* n, bool reset) override {
+        CK(cudaStreamSynchronize(stream));
+        for (auto& pe : ev_pending) {
+            float x = 0;
+            CK(cudaEventElapsedTime(&x, pe.second.first, pe.second.second));
+            t_ms[pe.first] += x;
+            t_n[pe.first] += 1;
+            ev_pool.push_back(pe.second.first);
+            ev_pool.push_back(pe.second.second);
+        }
+        ev_pending.clear();
+        if (ms) *ms = t_ms[k];
+        if (n) *n = t_n[k];
+        if (reset)
+            for (int j = 0; j < MPS_K_COUNT; ++j) { t_ms[j] = 0; t_n[j] = 0; }
+    }
 
     ~Solver() override {
         if (gexec) cudaGraphExecDestroy(gexec);
+        for (auto& pe : ev_pending) {
+            cudaEventDestroy(pe.second.first);
+            cudaEventDestroy(pe.second.second);
+        }
+        for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
         if (own_stream) {
             cudaStreamSynchronize(own_stream);
             cudaStreamDestroy(own_stream);
@@ -339,14 +412,14 @@ template <class R, class RN> class Solver final : public SolverBase {
             k_load_walls<R><<<blocks(nW, 256), 256, 0, stream>>>(nT, io.pos, io.vel, io.acc, io.typ,
                                                                  d_wall_ids, nW, tw_pos, tw_vel,
                                                                  tw_nrm, tw_id, tw_typ);
-            CKL();
+            KL();
             WallKeySrc<R, RN> ks{d_sc, nscene, dead(), tw_pos, tw_id};
             WallGather<R> g{tw_pos, tw_nrm, tw_vel, tw_id, tw_typ, w_pos, w_nrm, w_vel, w_id, w_typ};
             bin(ks, g, nullptr, nW, wcs);
             WallView<R> wl = wall_view();
             k_surface_edge<R, RN><<<blocks(nW, 128), 128, 0, stream>>>(d_sc, nscene, nW, wl, w_id,
                                                                        w_se);
-            CKL();
+            KL();
         } else {
             CK(cudaMemsetAsync(wcs, 0, sizeof(int) * (L() + 1), stream));
         }
@@ -422,26 +495,27 @@ template <class R, class RN> class Solver final : public SolverBase {
         if (n_max > 0) {
             int grid = std::min(blocks(n_max, 256), 148 * 32);
             k_bin_key<Src><<<grid, 256, 0, stream>>>(src, n_ptr, n_max, key, rnk, count, cnt);
-            CKL();
+            KL();
         }
         int nb = (L() + kScanTile - 1) / kScanTile;
         k_scan_reduce<<<nb, kScanThreads, 0, stream>>>(count, L(), part);
-        CKL();
+        KL();
         k_scan_apply<<<nb, kScanThreads, 0, stream>>>(count, L(), part, out_cs);
-        CKL();
+        KL();
         if (n_max > 0) {
             int grid = std::min(blocks(n_max, 256), 148 * 32);
             k_bin_seg<Src><<<grid, 256, 0, stream>>>(src, n_ptr, n_max, key, rnk, out_cs, seg);
-            CKL();
+            KL();
             k_bin_fin<Src, G><<<grid, 256, 0, stream>>>(src, g, n_ptr, n_max, key, rnk, out_cs, seg,
                                                         dead());
-            CKL();
+            KL();
         }
     }
 
     // fluid bucket build from (pos, vel, typ) sources into S2, then S <-> S2
     void bin_fluid(const V4<R>* pos, const V4<R>* vel, const V4<R>* acc, const R* prs,
                    const R* pav, const int* pid, const int8_t* typ) {
+        Scope sc_(this, MPS_K_BIN_FLUID);
         FluidKeySrc<R, RN> ks{d_sc, nscene, dead(), pos, typ, pid};
         FluidGather<R> g{pos, vel, acc, prs, pav, pid, typ,
                          S2.pos, S2.vel, S2.acc, S2.prs, S2.pav, S2.pid, S2.typ};
@@ -455,6 +529,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     }
 
     void bin_mirrors(MirrorBuf<R>& dst, int* dcs) {
+        Scope sc_(this, MPS_K_BIN_MIRROR);
         MirrorKeySrc<R, RN> ks{d_sc, nscene, dead(), U.pos, U.slot};
         MirrorGather<R> g{U.pos, U.slot, dst.pos, dst.slot};
         bin(ks, g, &cnt->mirror_raw, cap, dcs);
@@ -483,23 +558,39 @@ template <class R, class RN> class Solver final : public SolverBase {
     template <bool D> void fused_body() {
         const int gb = blocks(nF, block);
         // pass A: VscTrm + UpPcl1
-        k_pass_a<R, RN, D><<<gb, block, 0, stream>>>(args(M1, mcs1));
-        CKL();
+        {
+            Scope t(this, MPS_K_PASS_A);
+            k_pass_a<R, RN, D><<<gb, block, 0, stream>>>(args(M1, mcs1));
+            KL();
+        }
         // MkBkt on x* (kernel.cu:1917); the rebuild at kernel.cu:1921 would give the same lists
         bin_fluid(t_pos, t_vel, nullptr, S.prs, S.pav, S.pid, t_typ);
         // pass B: ChkCol + MkPrs, then the second mirror generation at (x*, P)
-        k_pass_b<R, RN, D><<<gb, block, 0, stream>>>(args(M1, mcs1));
-        CKL();
+        {
+            Scope t(this, MPS_K_PASS_B);
+            k_pass_b<R, RN, D><<<gb, block, 0, stream>>>(args(M1, mcs1));
+            KL();
+        }
         reset_raw();
-        k_gen_cull<R, RN><<<gb, block, 0, stream>>>(args(M1, mcs1), S.pos, t_prs, S.typ);
-        CKL();
+        {
+            Scope t(this, MPS_K_GEN);
+            // the step's second generation: the one the reference's counters would show last
+            k_gen_cull<R, RN, D><<<gb, block, 0, stream>>>(args(M1, mcs1), S.pos, t_prs, S.typ);
+            KL();
+        }
         bin_mirrors(M2, mcs2);
         // pass C: PrsGrdTrm + UpPcl2, then the first mirror generation of the next step
-        k_pass_c<R, RN, D><<<gb, block, 0, stream>>>(args(M2, mcs2));
-        CKL();
+        {
+            Scope t(this, MPS_K_PASS_C);
+            k_pass_c<R, RN, D><<<gb, block, 0, stream>>>(args(M2, mcs2));
+            KL();
+        }
         reset_raw();
-        k_gen_cull<R, RN><<<gb, block, 0, stream>>>(args(M2, mcs2), t_pos, t_prs, t_typ);
-        CKL();
+        {
+            Scope t(this, MPS_K_GEN);
+            k_gen_cull<R, RN, false><<<gb, block, 0, stream>>>(args(M2, mcs2), t_pos, t_prs, t_typ);
+            KL();
+        }
         bin_fluid(t_pos, t_vel, nullptr, t_prs, S.pav, S.pid, t_typ);
         bin_mirrors(M1, mcs1);
     }
@@ -513,9 +604,9 @@ template <class R, class RN> class Solver final : public SolverBase {
         }
         if (!m1_valid) {
             reset_raw();
-            k_gen_cull<R, RN><<<blocks(nF, block), block, 0, stream>>>(args(M1, mcs1), S.pos, S.prs,
-                                                                       S.typ);
-            CKL();
+            k_gen_cull<R, RN, false><<<blocks(nF, block), block, 0, stream>>>(args(M1, mcs1), S.pos,
+                                                                              S.prs, S.typ);
+            KL();
             bin_mirrors(M1, mcs1);
             m1_valid = true;
         }
@@ -538,10 +629,11 @@ template <class R, class RN> class Solver final : public SolverBase {
             run_body();
             ++done;
         }
-        if (graph_on && n - done > 0) {
+        if (graph_on && !timing_on && n - done > 0) {
             if (gexec && gexec_diag != diag_on) invalidate_graph();
             if (!gexec) {
                 cudaGraph_t g;
+                const long long l0 = launches;
                 CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
                 try {
                     run_body();
@@ -550,12 +642,17 @@ template <class R, class RN> class Solver final : public SolverBase {
                     throw;
                 }
                 CK(cudaStreamEndCapture(stream, &g));
+                body_launches = launches - l0;
+                launches = l0;  // captured, not yet run
                 cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
                 cudaGraphDestroy(g);
                 CK(e);
                 gexec_diag = diag_on;
             }
-            for (; done < n; ++done) CK(cudaGraphLaunch(gexec, stream));
+            for (; done < n; ++done) {
+                CK(cudaGraphLaunch(gexec, stream));
+                launches += body_launches;
+            }
         } else {
             for (; done < n; ++done) run_body();
         }
@@ -579,7 +676,7 @@ template <class R, class RN> class Solver final : public SolverBase {
                 if (nW > 0) {
                     k_surface_edge<R, RN><<<blocks(nW, 128), 128, 0, stream>>>(d_sc, nscene, nW,
                                                                                wall_view(), w_id, w_se);
-                    CKL();
+                    KL();
                 }
                 break;
             case MPS_PHASE_RESETMRR:
@@ -588,23 +685,23 @@ template <class R, class RN> class Solver final : public SolverBase {
             case MPS_PHASE_GENMRR_NONSLIP:
                 if (diag_on) k_ph_gen<R, RN, true><<<gb, block, 0, stream>>>(a);
                 else k_ph_gen<R, RN, false><<<gb, block, 0, stream>>>(a);
-                CKL();
+                KL();
                 break;
             case MPS_PHASE_MKBKT_MRR:
                 k_ph_cull<R, RN><<<std::min(blocks(cap, 256), 148 * 16), 256, 0, stream>>>(a);
-                CKL();
+                KL();
                 bin_mirrors(M1, mcs1);
                 break;
             case MPS_PHASE_VSCTRM:
                 need_lists();
                 if (diag_on) k_ph_vsc<R, RN, true><<<gb, block, 0, stream>>>(a);
                 else k_ph_vsc<R, RN, false><<<gb, block, 0, stream>>>(a);
-                CKL();
+                KL();
                 acc_dirty = true;
                 break;
             case MPS_PHASE_UPPCL1:
                 k_ph_uppcl1<R, RN><<<gb, block, 0, stream>>>(a);
-                CKL();
+                KL();
                 sorted = false;
                 acc_dirty = true;
                 break;
@@ -612,27 +709,27 @@ template <class R, class RN> class Solver final : public SolverBase {
                 need_lists();
                 if (diag_on) k_ph_col<R, RN, true><<<gb, block, 0, stream>>>(a);
                 else k_ph_col<R, RN, false><<<gb, block, 0, stream>>>(a);
-                CKL();
+                KL();
                 k_ph_upchkcol<R, RN><<<gb, block, 0, stream>>>(a);
-                CKL();
+                KL();
                 acc_dirty = true;
                 break;
             case MPS_PHASE_MKPRS:
                 need_lists();
                 if (diag_on) k_ph_prs<R, RN, true><<<gb, block, 0, stream>>>(a);
                 else k_ph_prs<R, RN, false><<<gb, block, 0, stream>>>(a);
-                CKL();
+                KL();
                 break;
             case MPS_PHASE_PRSGRDTRM:
                 need_lists();
                 if (diag_on) k_ph_grd<R, RN, true><<<gb, block, 0, stream>>>(a);
                 else k_ph_grd<R, RN, false><<<gb, block, 0, stream>>>(a);
-                CKL();
+                KL();
                 acc_dirty = true;
                 break;
             case MPS_PHASE_UPPCL2:
                 k_ph_uppcl2<R, RN><<<gb, block, 0, stream>>>(a);
-                CKL();
+                KL();
                 sorted = false;
                 acc_dirty = true;
                 break;
@@ -646,7 +743,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         k_load_fluid<R><<<blocks(nF, 256), 256, 0, stream>>>(io, d_fluid_ids, nF, S.pos, S.vel,
                                                              S.acc, S.prs, S.pav, S.pid, S.typ,
                                                              use_acc ? 1 : 0);
-        CKL();
+        KL();
         lists_valid = sorted = m1_valid = false;
         acc_dirty = use_acc;
     }
@@ -654,11 +751,11 @@ template <class R, class RN> class Solver final : public SolverBase {
     void store_all() {
         k_store_fluid<R, RN><<<blocks(nF, 256), 256, 0, stream>>>(io, d_sc, nscene, nF, S.pos, S.vel,
                                                                   S.acc, S.prs, S.pav, S.pid, S.typ);
-        CKL();
+        KL();
         if (nW > 0) {
             k_store_walls<R, RN><<<blocks(nW, 256), 256, 0, stream>>>(io, d_sc, nscene, nW, w_pos,
                                                                       w_vel, w_id, w_typ);
-            CKL();
+            KL();
         }
     }
 
@@ -776,6 +873,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         o->err_mirror_capacity = c.err_capacity;
         o->err_cell_range = c.err_cell;
         o->err_nan = c.err_nan;
+        o->kernel_launches = launches;
     }
 
     void integrals(int scene, double out[6]) override {
@@ -786,7 +884,7 @@ template <class R, class RN> class Solver final : public SolverBase {
                            stream));
         dim3 grid(std::min(blocks(std::max(nF, 1), 256), 148 * 4), nscene);
         k_integrals<R, RN><<<grid, 256, 0, stream>>>(d_sc, cs, S.pos, S.vel, S.typ, d_nbxyz, d_integ);
-        CKL();
+        KL();
         CK(cudaMemcpyAsync(init.data(), d_integ, sizeof(double) * init.size(), cudaMemcpyDeviceToHost,
                            stream));
         CK(cudaStreamSynchronize(stream));

@@ -17,7 +17,7 @@ import numpy as np
 from . import _lib as L
 from ._lib import MPSError, check, lib
 
-__all__ = ["MPS", "MPSBatch", "SceneDesc", "dambreak", "dambreak_params", "MPSError",
+__all__ = ["MPS", "MPSBatch", "SceneDesc", "dambreak", "dambreak_params", "derive", "select_device", "MPSError",
            "real_dtype"]
 
 
@@ -81,6 +81,18 @@ def dambreak_params(desc: SceneDesc, snd: float = 20.0, dt: float = 2e-4, nu: fl
         else:
             setattr(p, k, v)
     return p
+
+
+def select_device(device: int) -> None:
+    """Make `device` current for handles created by this thread (one process per GPU)."""
+    check(lib().mps_select_device(int(device)), "mps_select_device")
+
+
+def derive(params: L.mps_params) -> L.mps_info:
+    """Derived constants of a scene (host only, no GPU): AlcBkt + SetPara."""
+    inf = L.mps_info()
+    check(lib().mps_derive(C.byref(params), C.byref(inf)), "mps_derive")
+    return inf
 
 
 def _ptr(a):
@@ -159,10 +171,13 @@ class MPSBatch:
         check(lib().mps_get_info(self._h, scene, C.byref(inf)), "mps_get_info")
         return inf
 
-    def state(self) -> dict:
+    def state(self, out: dict | None = None) -> dict:
+        """DevicetoHost: the state in id order, into `out` (e.g. pinned buffers) if given."""
         n, dt = self.n, self.dtype
-        out = {"typ": np.empty(n, np.int8), "pos": np.empty((3, n), dt), "vel": np.empty((3, n), dt),
-               "acc": np.empty((3, n), dt), "prs": np.empty(n, dt), "pav": np.empty(n, dt)}
+        if out is None:
+            out = {"typ": np.empty(n, np.int8), "pos": np.empty((3, n), dt),
+                   "vel": np.empty((3, n), dt), "acc": np.empty((3, n), dt),
+                   "prs": np.empty(n, dt), "pav": np.empty(n, dt)}
         check(lib().mps_get_state(self._h, out["typ"].ctypes.data_as(L.c_int8_p), _ptr(out["pos"]),
                                   _ptr(out["vel"]), _ptr(out["acc"]), _ptr(out["prs"]),
                                   _ptr(out["pav"])), "mps_get_state")
@@ -207,7 +222,18 @@ class MPSBatch:
     def counters(self) -> dict:
         c = L.mps_counters()
         check(lib().mps_get_counters(self._h, C.byref(c)), "mps_get_counters")
-        return {k: getattr(c, k) for k, _ in L.mps_counters._fields_ if k != "reserved"}
+        return {k: getattr(c, k) for k, _ in L.mps_counters._fields_ if not k.startswith("reserved")}
+
+    def timing(self, reset: bool = False) -> dict:
+        """Per kernel group: (total device ms, launches) of the steps timed so far."""
+        out = {}
+        last = len(L.KERNEL_GROUPS) - 1
+        for k, name in enumerate(L.KERNEL_GROUPS):
+            ms, n = C.c_double(), C.c_int64()
+            rs = 1 if (reset and k == last) else 0  # read every group before clearing
+            check(lib().mps_get_timing(self._h, k, C.byref(ms), C.byref(n), rs), "mps_get_timing")
+            out[name] = (ms.value, n.value)
+        return out
 
     def integrals(self, scene: int = 0) -> np.ndarray:
         out = (C.c_double * 6)()

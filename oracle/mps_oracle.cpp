@@ -789,6 +789,9 @@ int oracle_set_state(void* h, const int8_t* typ, const void* pos, const void* ve
         get3(o.ax, o.ay, o.az, acc);
         if (prs) std::copy(static_cast<const R*>(prs), static_cast<const R*>(prs) + o.n, o.prs.begin());
         if (pav) std::copy(static_cast<const R*>(pav), static_cast<const R*>(pav) + o.n, o.pav.begin());
+        // every method of the reference that reads the bucket lists runs after an MkBkt on
+        // the same positions, so a replaced state gets fresh lists
+        o.mkbkt();
         return 0;
     });
 }

@@ -1,0 +1,153 @@
+"""Scene generator, parameter helper and the C-ABI surface (no GPU needed)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from mps_cuda_b200 import F32, F64, SceneDesc, configs, dambreak, dambreak_params, derive
+from mps_cuda_b200 import _lib as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "mps_b200.h")
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(mps_\w+)\s*\(", txt, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    out = subprocess.run(["nm", "-D", "--defined-only", L.library_path()], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (mps_\w+)", out))
+    missing = [s for s in syms if s not in exported]
+    assert not missing, missing
+    # and the ctypes binding declares a signature for each
+    assert sorted(L.SIGNATURES) == syms
+    lib = L.lib()
+    for s in syms:
+        assert hasattr(lib, s)
+
+
+def test_status_strings():
+    lib = L.lib()
+    for code in range(9):
+        assert lib.mps_status_string(code)
+    assert lib.mps_status_string(99) == b"unknown status"
+
+
+def test_argument_errors_without_gpu():
+    lib = L.lib()
+    p = L.mps_params()
+    inf = L.mps_info()
+    assert lib.mps_derive(C.byref(p), C.byref(inf)) == L.MPS_ERR_ARG  # l0 = 0
+    assert b"positive" in lib.mps_last_error()
+    d = SceneDesc(0.02, (0.4, 0.2, 0.4), (4, 4, 4)).c()
+    typ = np.empty(10, np.int8)
+    buf = np.empty(30)
+    n = C.c_int32()
+    rc = lib.mps_scene_dambreak(C.byref(d), 10, typ.ctypes.data_as(L.c_int8_p),
+                                buf.ctypes.data_as(L.c_double_p), buf.ctypes.data_as(L.c_double_p),
+                                buf.ctypes.data_as(L.c_double_p), C.byref(n))
+    assert rc == L.MPS_ERR_ARG and n.value > 10
+    assert lib.mps_step(None, 1) == L.MPS_ERR_ARG
+    assert lib.mps_destroy(None) == L.MPS_OK
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-device status")
+def test_create_without_device_reports_nodevice():
+    desc = SceneDesc(0.02, (0.4, 0.2, 0.4), (2, 2, 2))
+    sc = dambreak(desc)
+    p = dambreak_params(desc, precision=F64)
+    h = C.c_void_p()
+    rc = L.lib().mps_create(C.byref(p), sc["typ"].shape[0], sc["typ"].ctypes.data_as(L.c_int8_p),
+                            sc["pos"].ctypes.data_as(C.c_void_p), sc["vel"].ctypes.data_as(C.c_void_p),
+                            sc["nrm"].ctypes.data_as(C.c_void_p), C.byref(h))
+    assert rc == L.MPS_ERR_NODEVICE and not h.value
+
+
+def test_dambreak_counts_and_layout():
+    desc, _, _ = configs.WORKLOADS["dambreak_l0.02_6k"]
+    sc = dambreak(desc)
+    typ, pos, nrm = sc["typ"], sc["pos"], sc["nrm"]
+    nf = int((typ == 0).sum())
+    assert nf == 20 * 10 * 30
+    nx, ny, nz = 50, 10, 40
+    assert int((typ == 1).sum()) == 2 * ny * nz + 2 * nx * nz + nx * ny
+    assert np.all(typ[:nf] == 0) and np.all(typ[nf:] == 1)
+    w = typ == 1
+    # unit normals pointing into the tank; every wall particle on its face plane
+    assert np.allclose(np.linalg.norm(nrm[:, w], axis=0), 1.0)
+    assert np.all(nrm[:, ~w] == 0)
+    for ax, L_ in enumerate((1.0, 0.2, 0.8)):
+        on = w & (np.abs(nrm[ax]) == 1)
+        plane = np.where(nrm[ax, on] > 0, 0.0, L_)
+        assert np.allclose(pos[ax, on], plane)
+    # in-plane positions at half-integer multiples of l0
+    frac = (pos[:, w] / 0.02) % 1.0
+    onplane = np.abs(nrm[:, w]) == 1
+    assert np.allclose(frac[~onplane], 0.5)
+
+
+def test_dambreak_jitter_is_bounded_and_seeded():
+    desc = SceneDesc(0.02, (0.4, 0.2, 0.4), (5, 4, 6), seed=7)
+    a, b = dambreak(desc), dambreak(desc)
+    assert np.array_equal(a["pos"], b["pos"])
+    c = dambreak(SceneDesc(0.02, (0.4, 0.2, 0.4), (5, 4, 6), seed=8))
+    assert not np.array_equal(a["pos"], c["pos"])
+    nf = 5 * 4 * 6
+    base = (np.round(a["pos"][:, :nf] / 0.02 - 0.5) + 0.5) * 0.02
+    dev = np.abs(a["pos"][:, :nf] - base)
+    assert dev.max() <= 0.01 * 0.02 + 1e-15 and dev.max() > 0.005 * 0.02
+
+
+def test_initial_velocity_distribution():
+    desc, _, _ = configs.WORKLOADS["adjoint_l0.01_48k"]
+    sc = dambreak(desc)
+    v = sc["vel"][:, sc["typ"] == 0]
+    assert v.shape[1] == 48000
+    assert abs(v.mean()) < 2e-3 and abs(v.std() - 0.05) < 1e-3
+
+
+def test_params_dambreak():
+    desc = SceneDesc(0.02, (1.0, 0.2, 0.8), (20, 10, 30))
+    p = dambreak_params(desc, snd=20.0, dt=2e-4, nu=1e-6, precision=F32)
+    H = 29 * 0.02
+    assert p.umax == pytest.approx(np.sqrt(2 * 9.81 * H))
+    assert p.pmax == pytest.approx(1000 * 9.81 * H)
+    assert list(p.g) == [0.0, 0.0, -9.81] and p.rho == 1000.0 and p.snd == 20.0
+    inf = derive(p)
+    assert inf.prs_coef == pytest.approx(400.0 / inf.n0_grad, rel=1e-6)
+    assert inf.rlim2 == pytest.approx((0.9 * 0.02) ** 2, rel=1e-6)
+    assert inf.col == pytest.approx(1.2)
+
+
+def test_batched_scene_draws():
+    scenes = configs.batched_scenes()
+    assert len(scenes) == 64
+    counts = []
+    for desc, dt in scenes:
+        nf = int(np.prod(desc.block))
+        assert 2000 <= nf <= 60000
+        assert desc.l0 in (0.01, 0.015, 0.02)
+        assert 1.0 <= desc.tank[0] <= 1.6
+        assert 0 < dt < 0.25 * desc.l0 / 20.0
+        counts.append(nf)
+    assert len(set(counts)) > 30  # uneven sizes
+    again = configs.batched_scenes()
+    assert [d.block for d, _ in again] == [d.block for d, _ in scenes]

@@ -277,6 +277,33 @@ int mps_get_timing(mps_handle* h, int32_t kernel, double* total_ms, int64_t* lau
  */
 int mps_get_integrals(mps_handle* h, int32_t scene, double out[6]);
 
+/* ---- bucket build without allocation ---------------------------------------------- */
+
+#define MPS_NOALLOC_MAX_ITEMS (1 << 20)   /* particles per call                         */
+#define MPS_NOALLOC_MAX_BUCKETS (1 << 20) /* buckets of the scene's grid                 */
+
+/*
+ * MkBkt (kernel.cu:516-550) for callers that cannot allocate device memory, such as code
+ * running inside another framework's memory pool, real-time loops that must not allocate
+ * after start-up, or plug-ins handed only their input and output buffers. No counterpart in
+ * the reference: it has no such entry point. Every temporary lives in one fixed array of
+ * about 21 MB inside the library (held on every GPU that loads it, until exit), so nothing
+ * is allocated per call; the caller passes device buffers:
+ *   typ[n], pos (SoA x[n], y[n], z[n]; float, or double for MPS_F64) - inputs;
+ *   cell[n]       bucket index ib of each particle, -1 for GST          - output;
+ *   order[n]      ids of the non-GST particles sorted by (bucket, id); entries past
+ *                 start[nbxyz] are left untouched                        - output;
+ *   start[nbxyz+1] first position in `order` of every bucket             - output.
+ * nbxyz is the grid size of `p` (mps_derive). Work is queued on `stream` (a cudaStream_t,
+ * NULL = legacy default) and not synchronised. Sizes above MPS_NOALLOC_MAX_ITEMS particles
+ * or MPS_NOALLOC_MAX_BUCKETS buckets are rejected with MPS_ERR_OVERFLOW. All calls on a
+ * device share the array: calls whose work overlaps on the GPU race, so serialise them on
+ * one stream. The first call on a device looks up the array's address there; make it
+ * before any stream capture.
+ */
+int mps_bucket_build_noalloc(const mps_params* p, int32_t n, const int8_t* typ, const void* pos,
+                             int32_t* cell, int32_t* order, int32_t* start, void* stream);
+
 /* ---- errors ----------------------------------------------------------------------- */
 const char* mps_status_string(int32_t status);
 /* Text of the last failure on this thread (CUDA error string, argument check, ...). */

@@ -25,6 +25,8 @@ MPS_ERR_OVERFLOW, MPS_ERR_TIMEOUT, MPS_ERR_UNSUPPORTED, MPS_ERR_NODEVICE = 5, 6,
 GST, FLD, WLL, OBJ, OBJ2, MRR = -1, 0, 1, 2, 3, 4
 SURFACE, EDGE = 0, 1
 NUM_MRR = 10
+NOALLOC_MAX_ITEMS = 1 << 20
+NOALLOC_MAX_BUCKETS = 1 << 20
 F32, F64, F32_N64 = 0, 1, 2
 (PHASE_MKBKT, PHASE_SURFACE_EDGE, PHASE_RESETMRR, PHASE_GENMRR_NONSLIP, PHASE_MKBKT_MRR,
  PHASE_VSCTRM, PHASE_UPPCL1, PHASE_CHKCOL, PHASE_MKPRS, PHASE_PRSGRDTRM, PHASE_UPPCL2) = range(11)
@@ -100,6 +102,9 @@ SIGNATURES = {
     "mps_get_timing": (C.c_int, [C.c_void_p, C.c_int32, c_double_p, C.POINTER(C.c_int64),
                                  C.c_int32]),
     "mps_get_integrals": (C.c_int, [C.c_void_p, C.c_int32, c_double_p]),
+    "mps_bucket_build_noalloc": (C.c_int, [C.POINTER(mps_params), C.c_int32, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p]),
     "mps_status_string": (C.c_char_p, [C.c_int32]),
     "mps_last_error": (C.c_char_p, []),
 }

@@ -20,7 +20,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmps_b200.so")
-SOURCES = ["mps_api.cu", "mps_inst_f32.cu", "mps_inst_f64.cu", "mps_inst_mix.cu", "mps_scene.cpp"]
+SOURCES = ["mps_api.cu", "mps_inst_f32.cu", "mps_inst_f64.cu", "mps_inst_mix.cu",
+           "mps_noalloc.cu", "mps_scene.cpp"]
 HEADERS = ["mps_types.h", "mps_device.cuh", "mps_kernels.cuh", "mps_solver.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -110,6 +110,27 @@ __device__ __forceinline__ void for_rows(const SceneDev<R, RN>& sc, const int* _
     }
 }
 
+// for_rows, handing each (trimmed) row range [lo, hi) to f(lo, hi) in visiting order
+template <class R, class RN, class F>
+__device__ __forceinline__ void for_rows_ranges(const SceneDev<R, RN>& sc,
+                                                const int* __restrict__ cs, const RowCtx<R>& c,
+                                                R B, F&& f) {
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz) {
+        R ddz = dz < 0 ? c.dzl : (dz > 0 ? c.dzh : R(0));
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+            R ddy = dy < 0 ? c.dyl : (dy > 0 ? c.dyh : R(0));
+            R dyz2 = ddy * ddy + ddz * ddz;
+            if (dyz2 > B) continue;
+            int jl = (dyz2 + c.dxl * c.dxl <= B) ? c.ix - 1 : c.ix;
+            int jh = (dyz2 + c.dxh * c.dxh <= B) ? c.ix + 1 : c.ix;
+            int row = sc.cbase + (c.iz + dz) * sc.nbxy + (c.iy + dy) * sc.nbx;
+            f(__ldg(cs + row + jl), __ldg(cs + row + jh + 1));
+        }
+    }
+}
+
 // ---- views ------------------------------------------------------------------------------
 template <class R> struct WallView {
     const int* cs;
@@ -207,14 +228,18 @@ __device__ __forceinline__ void col_hit(R colfac, R ux, R uy, R uz, R jx, R jy, 
 }
 
 template <class R, class RN>
-__device__ __forceinline__ void dens_add(const SceneDev<R, RN>& sc, R d2, RN& ni) {
+__device__ __forceinline__ void dens_add_v(R rp, RN rp_n, R d2, RN& ni) {
     if (sizeof(RN) == sizeof(R)) {
         R d = sqrtR(d2);
-        ni += RN(wei_grad(d, sc.rp));
+        ni += RN(wei_grad(d, rp));
     } else {
         RN d = sqrtR(RN(d2));
-        ni += wei_grad(d, sc.rp_n);
+        ni += wei_grad(d, rp_n);
     }
+}
+template <class R, class RN>
+__device__ __forceinline__ void dens_add(const SceneDev<R, RN>& sc, R d2, RN& ni) {
+    dens_add_v(sc.rp, sc.rp_n, d2, ni);
 }
 
 // wall (collision only) and mirror parts, visited after the fluid neighbours
@@ -356,6 +381,17 @@ __device__ __forceinline__ void grad_sum(const SceneDev<R, RN>& sc, const RowCtx
         }
     });
     grad_sum_mirrors(sc, c, pid_local, x, y, z, pmin, m, skip, sx, sy, sz, cm);
+}
+
+// out-of-line copy for the rare slot whose neighbour list overflowed its capacity
+template <class R, class RN>
+__device__ __noinline__ void grad_sum_outline(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
+                                              int pid_local, R x, R y, R z, R pi,
+                                              const int* __restrict__ cs,
+                                              const V4<R>* __restrict__ pos,
+                                              const R* __restrict__ prs, const MirrorView<R>& m,
+                                              bool skip, R& sx, R& sy, R& sz, int& cf, int& cm) {
+    grad_sum(sc, c, s, pid_local, x, y, z, pi, cs, pos, prs, m, skip, sx, sy, sz, cf, cm);
 }
 
 // ---- MRRinout cull of one mirror (kernel.cu:932-985); true = keep -----------------------

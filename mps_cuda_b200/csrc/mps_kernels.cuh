@@ -270,7 +270,31 @@ template <class R, class RN> struct PassArgs {
     int* nb;
     int* nbcnt;
     int nbK;
+    const int8_t* near_wall;  // per bucket: a wall lies in the 27 buckets around it
 };
+
+// near_wall flag of every bucket of every scene (walls are static: computed once)
+template <class R, class RN>
+__global__ void k_near_wall(const SceneDev<R, RN>* scs, int nscene, const int* __restrict__ wcs,
+                            int8_t* near_wall) {
+    const int sidx = blockIdx.y;
+    const SceneDev<R, RN>& sc = scs[sidx];
+    const int nb = sc.nbxy * sc.nbz;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        const int iz = b / sc.nbxy, iy = (b % sc.nbxy) / sc.nbx, ix = b % sc.nbx;
+        int8_t f = 1;  // buckets on the grid border hold no particle: keep them conservative
+        if (ix >= 1 && ix <= sc.nbx - 2 && iy >= 1 && iy <= sc.nby - 2 && iz >= 1 &&
+            iz <= sc.nbz - 2) {
+            f = 0;
+            for (int dz = -1; dz <= 1; ++dz)
+                for (int dy = -1; dy <= 1; ++dy) {
+                    const int row = sc.cbase + (iz + dz) * sc.nbxy + (iy + dy) * sc.nbx;
+                    if (wcs[row + ix + 2] > wcs[row + ix - 1]) f = 1;
+                }
+        }
+        near_wall[sc.cbase + b] = f;
+    }
+}
 
 template <class R, class RN>
 __device__ __forceinline__ const SceneDev<R, RN>& scene_ref(const PassArgs<R, RN>& a, int pid) {
@@ -286,16 +310,28 @@ __device__ __forceinline__ int build_list(const PassArgs<R, RN>& a, const SceneD
                                           const RowCtx<R>& c, int s, R x, R y, R z, R thr, R B) {
     int cnt = 0;
     int* __restrict__ nb = a.nb;
+    const V4<R>* __restrict__ pos = a.pos;
     const int nF = a.nF, K = a.nbK;
-    for_rows(sc, a.cs, c, B, [&](int j) {
-        if (j == s) return;
-        V4<R> q = ldg4(a.pos + j);
-        R dx = q.x - x, dy = q.y - y, dz = q.z - z;
-        R d2 = dot3(dx, dy, dz, dx, dy, dz);
-        if (d2 <= thr) {
-            if (cnt < K) nb[size_t(cnt) * nF + s] = j;
-            ++cnt;
+    for_rows_ranges(sc, a.cs, c, B, [&](int lo, int hi) {
+        // four independent loads in flight before the first test (latency, not bandwidth,
+        // bounds this loop); candidates are still tested and appended in slot order
+        int j = lo;
+        auto visit = [&](int jj, const V4<R>& q) {
+            R dx = q.x - x, dy = q.y - y, dz = q.z - z;
+            if (jj != s && dot3(dx, dy, dz, dx, dy, dz) <= thr) {
+                if (cnt < K) nb[size_t(cnt) * nF + s] = jj;
+                ++cnt;
+            }
+        };
+        for (; j + 4 <= hi; j += 4) {
+            V4<R> q0 = ldg4(pos + j), q1 = ldg4(pos + j + 1), q2 = ldg4(pos + j + 2),
+                  q3 = ldg4(pos + j + 3);
+            visit(j, q0);
+            visit(j + 1, q1);
+            visit(j + 2, q2);
+            visit(j + 3, q3);
         }
+        for (; j < hi; ++j) visit(j, ldg4(pos + j));
     });
     return cnt;
 }
@@ -322,16 +358,30 @@ __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
     int cf = 0, cm = 0;
     const int n = build_list(a, sc, c, s, p.x, p.y, p.z, sc.r_le, MPS_INF_SKIP(a, sc.skip_r));
     if (n <= a.nbK) {
-        for (int k = 0; k < n; ++k) {
-            const int j = a.nb[size_t(k) * a.nF + s];
-            V4<R> q = ldg4(a.pos + j), u = ldg4(a.vel + j);
+        const int* __restrict__ nb = a.nb + s;
+        const V4<R>* __restrict__ pos = a.pos;
+        const V4<R>* __restrict__ vel = a.vel;
+        const size_t st = a.nF;
+        const R two_l0 = sc.two_l0;
+        auto add = [&](const V4<R>& q, const V4<R>& u) {
             R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
             R d2 = dot3(dx, dy, dz, dx, dy, dz);
             R d = sqrtR(d2);
-            R w = sc.two_l0 / (d2 * d);
+            R w = two_l0 / (d2 * d);
             sx = fmaR(u.x - v.x, w, sx);
             sy = fmaR(u.y - v.y, w, sy);
             sz = fmaR(u.z - v.z, w, sz);
+        };
+        int k = 0;
+        for (; k + 2 <= n; k += 2) {  // two neighbours' loads in flight, summed in order
+            const int j0 = nb[k * st], j1 = nb[(k + 1) * st];
+            V4<R> q0 = ldg4(pos + j0), u0 = ldg4(vel + j0), q1 = ldg4(pos + j1), u1 = ldg4(vel + j1);
+            add(q0, u0);
+            add(q1, u1);
+        }
+        if (k < n) {
+            const int j = nb[k * st];
+            add(ldg4(pos + j), ldg4(vel + j));
         }
         cf = n;
         visc_sum_mirrors(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.m, MPS_INF_SKIP(a, sc.skip_r), sx, sy,
@@ -382,20 +432,38 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
     const int n = build_list(a, sc, c, s, p.x, p.y, p.z, sc.list_thr, MPS_INF_SKIP(a, sc.skip_rc));
     a.nbcnt[s] = n;
     if (n <= a.nbK) {
-        for (int k = 0; k < n; ++k) {
-            const int j = a.nb[size_t(k) * a.nF + s];
-            V4<R> q = ldg4(a.pos + j);
+        const int* __restrict__ nb = a.nb + s;
+        const V4<R>* __restrict__ pos = a.pos;
+        const V4<R>* __restrict__ vel = a.vel;
+        const size_t st = a.nF;
+        const R rlim2 = sc.rlim2, rp_lt = sc.rp_lt, colfac = sc.colfac, rp = sc.rp;
+        const RN rp_n = sc.rp_n;
+        auto add = [&](int j, const V4<R>& q) {
             R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
             R d2 = dot3(dx, dy, dz, dx, dy, dz);
-            if (d2 < sc.rlim2) {
-                V4<R> u = ldg4(a.vel + j);
-                col_hit(sc.colfac, v.x, v.y, v.z, u.x, u.y, u.z, dx, dy, dz, d2, wx, wy, wz);
+            if (d2 < rlim2) {
+                V4<R> u = ldg4(vel + j);
+                col_hit(colfac, v.x, v.y, v.z, u.x, u.y, u.z, dx, dy, dz, d2, wx, wy, wz);
                 ++cnt5[0];
             }
-            if (d2 <= sc.rp_lt) {
-                dens_add(sc, d2, ni);
+            if (d2 <= rp_lt) {
+                dens_add_v(rp, rp_n, d2, ni);
                 ++cnt5[3];
             }
+        };
+        int k = 0;
+        for (; k + 4 <= n; k += 4) {
+            const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
+                      j3 = nb[(k + 3) * st];
+            V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
+            add(j0, q0);
+            add(j1, q1);
+            add(j2, q2);
+            add(j3, q3);
+        }
+        for (; k < n; ++k) {
+            const int j = nb[k * st];
+            add(j, ldg4(pos + j));
         }
         col_dens_walls_mirrors<R, RN, true, true>(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.wl, a.m,
                                                   a.skip != 0, wx, wy, wz, ni, cnt5);
@@ -440,37 +508,65 @@ __global__ void __launch_bounds__(128) k_pass_c(PassArgs<R, RN> a) {
     int cf = 0, cm = 0;
     const int n = a.nbcnt[s];
     if (n <= a.nbK) {
+        const int* __restrict__ nb = a.nb + s;
+        const V4<R>* __restrict__ pos = a.pos;
+        const R* __restrict__ prs = a.tprs;
+        const size_t st = a.nF;
+        const R rp2 = sc.rp2, rp = sc.rp;
+        // P_min over the fluid neighbours inside rp (order-free), then the gradient in order
         R pmin = pi;
-        for (int k = 0; k < n; ++k) {
-            const int j = a.nb[size_t(k) * a.nF + s];
-            V4<R> q = ldg4(a.pos + j);
+        auto mn = [&](int j, const V4<R>& q) {
             R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-            R d2 = dot3(dx, dy, dz, dx, dy, dz);
-            if (d2 < sc.rp2) {
-                R pj = __ldg(a.tprs + j);
+            if (dot3(dx, dy, dz, dx, dy, dz) < rp2) {
+                R pj = __ldg(prs + j);
                 if (pj < pmin) pmin = pj;
             }
+        };
+        int k = 0;
+        for (; k + 4 <= n; k += 4) {
+            const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
+                      j3 = nb[(k + 3) * st];
+            V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
+            mn(j0, q0);
+            mn(j1, q1);
+            mn(j2, q2);
+            mn(j3, q3);
         }
-        for (int k = 0; k < n; ++k) {
-            const int j = a.nb[size_t(k) * a.nF + s];
-            V4<R> q = ldg4(a.pos + j);
+        for (; k < n; ++k) {
+            const int j = nb[k * st];
+            mn(j, ldg4(pos + j));
+        }
+        auto gr = [&](int j, const V4<R>& q) {
             R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
             R d2 = dot3(dx, dy, dz, dx, dy, dz);
-            if (d2 < sc.rp2) {
+            if (d2 < rp2) {
                 R d = sqrtR(d2);
-                R w = wei_grad(d, sc.rp) / d2;
-                R pw = (__ldg(a.tprs + j) - pmin) * w;
+                R w = wei_grad(d, rp) / d2;
+                R pw = (__ldg(prs + j) - pmin) * w;
                 sx = fmaR(pw, dx, sx);
                 sy = fmaR(pw, dy, sy);
                 sz = fmaR(pw, dz, sz);
                 ++cf;
             }
+        };
+        for (k = 0; k + 4 <= n; k += 4) {
+            const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
+                      j3 = nb[(k + 3) * st];
+            V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
+            gr(j0, q0);
+            gr(j1, q1);
+            gr(j2, q2);
+            gr(j3, q3);
+        }
+        for (; k < n; ++k) {
+            const int j = nb[k * st];
+            gr(j, ldg4(pos + j));
         }
         grad_sum_mirrors(sc, c, pid - sc.pbase, p.x, p.y, p.z, pmin, a.m, a.skip != 0, sx, sy, sz,
                          cm);
     } else {
-        grad_sum(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, pi, a.cs, a.pos, a.tprs, a.m,
-                 a.skip != 0, sx, sy, sz, cf, cm);
+        grad_sum_outline(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, pi, a.cs, a.pos, a.tprs, a.m,
+                         a.skip != 0, sx, sy, sz, cf, cm);
     }
     R ax = (sc.invro * sx) * sc.a3, ay = (sc.invro * sy) * sc.a3, az = (sc.invro * sz) * sc.a3;
     V4<R> v = a.tvel[s];
@@ -497,7 +593,7 @@ __global__ void __launch_bounds__(128) k_pass_c(PassArgs<R, RN> a) {
 // of a step (x*, P after pass B) and the first generation of the next one (x^{n+1}, P after
 // pass C). Near-wall particles are a thin layer, so this runs as a light kernel of its own
 // instead of stretching the neighbour passes.
-template <class R, class RN, bool DIAG>
+template <class R, class RN, bool DIAG, bool CULL>
 __global__ void __launch_bounds__(128) k_gen_cull(PassArgs<R, RN> a, const V4<R>* gpos,
                                                   const R* gprs, const int8_t* gtyp) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -507,8 +603,13 @@ __global__ void __launch_bounds__(128) k_gen_cull(PassArgs<R, RN> a, const V4<R>
     V4<R> p = gpos[s];
     int ix, iy, iz;
     cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    // no wall in the 27 buckets around: no wall within r, no mirror (the common case)
+    if (!__ldg(a.near_wall + sc.cbase + iz * sc.nbxy + iy * sc.nbx + ix)) {
+        if (DIAG) a.diag[size_t(pid) * kDiagCols + DG_GEN_W] = 0;
+        return;
+    }
     RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
-    int nw = gen_mirrors<R, RN, true>(sc, c, p.x, p.y, p.z, gprs[s], pid * kNumMRR, a.wl,
+    int nw = gen_mirrors<R, RN, CULL>(sc, c, p.x, p.y, p.z, gprs[s], pid * kNumMRR, a.wl,
                                       a.skip != 0, a.out, a.cnt);
     if (DIAG) a.diag[size_t(pid) * kDiagCols + DG_GEN_W] = nw;
 }

@@ -254,6 +254,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     double* d_integ;
     int* nb;
     int* nbcnt;
+    int8_t* near_wall;
     int nbK = 160;  // list capacity: about 125 neighbours lie inside r at rest density
     std::vector<int> fluid_ids, wall_ids;
     bool lists_valid = false, sorted = false, m1_valid = false, acc_dirty = false;
@@ -423,6 +424,11 @@ template <class R, class RN> class Solver final : public SolverBase {
         } else {
             CK(cudaMemsetAsync(wcs, 0, sizeof(int) * (L() + 1), stream));
         }
+        {
+            dim3 g(std::max(1, std::min(blocks(C, 256), 148 * 4)), nscene);
+            k_near_wall<R, RN><<<g, 256, 0, stream>>>(d_sc, nscene, wcs, near_wall);
+            KL();
+        }
         load_fluid(false);
         mkbkt(true);
         CK(cudaStreamSynchronize(stream));
@@ -481,6 +487,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         io.cell = ar.template get<int>(T);
         d_integ = ar.template get<double>(6 * size_t(nscene));
         nb = ar.template get<int>(size_t(nbK) * F);
+        near_wall = ar.template get<int8_t>(L());
         nbcnt = ar.template get<int>(F);
         CK(cudaMemsetAsync(S.acc, 0, sizeof(V4<R>) * F, stream));
         CK(cudaMemsetAsync(S2.acc, 0, sizeof(V4<R>) * F, stream));
@@ -550,10 +557,18 @@ template <class R, class RN> class Solver final : public SolverBase {
         a.out = MirrorSink<R>{U.pos, U.slot, cap};
         a.cnt = cnt; a.diag = diag; a.ndens = ndens;
         a.nb = nb; a.nbcnt = nbcnt; a.nbK = nbK;
+        a.near_wall = near_wall;
         return a;
     }
 
     void reset_raw() { CK(cudaMemsetAsync(&cnt->mirror_raw, 0, sizeof(int), stream)); }
+
+    // MRRinout over the raw mirrors, one thread per mirror (culled slots turn negative)
+    void cull_raw() {
+        k_ph_cull<R, RN><<<std::min(blocks(cap, 256), 148 * 16), 256, 0, stream>>>(args(M1, mcs1));
+        KL();
+    }
+
 
     template <bool D> void fused_body() {
         const int gb = blocks(nF, block);
@@ -575,8 +590,10 @@ template <class R, class RN> class Solver final : public SolverBase {
         {
             Scope t(this, MPS_K_GEN);
             // the step's second generation: the one the reference's counters would show last
-            k_gen_cull<R, RN, D><<<gb, block, 0, stream>>>(args(M1, mcs1), S.pos, t_prs, S.typ);
+            k_gen_cull<R, RN, D, false><<<gb, block, 0, stream>>>(args(M1, mcs1), S.pos, t_prs,
+                                                                  S.typ);
             KL();
+            cull_raw();
         }
         bin_mirrors(M2, mcs2);
         // pass C: PrsGrdTrm + UpPcl2, then the first mirror generation of the next step
@@ -588,8 +605,10 @@ template <class R, class RN> class Solver final : public SolverBase {
         reset_raw();
         {
             Scope t(this, MPS_K_GEN);
-            k_gen_cull<R, RN, false><<<gb, block, 0, stream>>>(args(M2, mcs2), t_pos, t_prs, t_typ);
+            k_gen_cull<R, RN, false, false><<<gb, block, 0, stream>>>(args(M2, mcs2), t_pos, t_prs,
+                                                                      t_typ);
             KL();
+            cull_raw();
         }
         bin_fluid(t_pos, t_vel, nullptr, t_prs, S.pav, S.pid, t_typ);
         bin_mirrors(M1, mcs1);
@@ -604,9 +623,10 @@ template <class R, class RN> class Solver final : public SolverBase {
         }
         if (!m1_valid) {
             reset_raw();
-            k_gen_cull<R, RN, false><<<blocks(nF, block), block, 0, stream>>>(args(M1, mcs1), S.pos,
-                                                                              S.prs, S.typ);
+            k_gen_cull<R, RN, false, false><<<blocks(nF, block), block, 0, stream>>>(
+                args(M1, mcs1), S.pos, S.prs, S.typ);
             KL();
+            cull_raw();
             bin_mirrors(M1, mcs1);
             m1_valid = true;
         }
@@ -688,8 +708,7 @@ template <class R, class RN> class Solver final : public SolverBase {
                 KL();
                 break;
             case MPS_PHASE_MKBKT_MRR:
-                k_ph_cull<R, RN><<<std::min(blocks(cap, 256), 148 * 16), 256, 0, stream>>>(a);
-                KL();
+                cull_raw();
                 bin_mirrors(M1, mcs1);
                 break;
             case MPS_PHASE_VSCTRM:

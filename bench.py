@@ -312,6 +312,9 @@ def run_ours(args, world, rank, local):
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": 1e3 * el / K}
 
+    batched = None
+    if not args.no_batched:
+        batched = measure_batched(args, stream, flush, min(K, 50))
     clk.__exit__(None, None, None)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -332,10 +335,74 @@ def run_ours(args, world, rank, local):
             "clocks": clk.summary(), "wall_ms_per_step": 1e3 * wall / K,
             "e2e": e2e, "gpu_launches": launches,
             "roofline": roofline, "kernel_groups": groups, "cpu_baseline": cpu,
+            "batched": batched,
             "counters": {k: v for k, v in cnt.items() if k != "kernel_launches"},
         }
         print(json.dumps(line), flush=True)
     g.close()
+
+
+def measure_batched(args, stream, flush, K: int):
+    """64 uneven dam breaks (FP32 state, FP64 number density, per-scene dt from CFL 0.2):
+    one handle advancing all scenes per graph launch vs the per-scene loop (64 handles, one
+    graph launch each per step, on the same stream). Device time, L2 flushed between steps."""
+    import torch
+
+    from mps_cuda_b200 import F32_N64, MPS, MPSBatch, configs, dambreak, dambreak_params
+    from mps_cuda_b200 import _lib as L
+
+    scenes = configs.batched_scenes()
+    parts, params = [], []
+    for desc, dt in scenes:
+        sc = dambreak(desc)
+        parts.append(sc)
+        params.append(dambreak_params(desc, dt=dt, precision=F32_N64))
+    counts = [p_["typ"].shape[0] for p_ in parts]
+    nfl = sum(int((p_["typ"] == 0).sum()) for p_ in parts)
+    cat = lambda k: np.concatenate([p_[k] for p_ in parts], axis=-1)
+    f32 = lambda a: a.astype(np.float32)
+
+    def timed(step_fn):
+        e0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        e1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            for k in range(K):
+                flush.fill_(float(k))
+                e0[k].record(stream)
+                step_fn()
+                e1[k].record(stream)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in zip(e0, e1))
+
+    b = MPSBatch(params, cat("typ"), f32(cat("pos")), f32(cat("vel")), f32(cat("nrm")), counts=counts)
+    b.set_stream(stream.cuda_stream)
+    tuned = b.autotune(3)
+    b.set_option(L.OPT_GRAPH, 1)
+    b.step(3)
+    ms_batch = timed(lambda: b.step(1))
+    hs = []
+    for pp, pt in zip(params, parts):
+        h = MPS(pp, pt["typ"], f32(pt["pos"]), f32(pt["vel"]), f32(pt["nrm"]))
+        h.set_stream(stream.cuda_stream)
+        h.set_option(L.OPT_GRAPH, 1)
+        h.step(3)
+        hs.append(h)
+
+    def loop():
+        for h in hs:
+            h.step(1)
+    ms_loop = timed(loop)
+    for h in hs:
+        h.close()
+    b.close()
+    return {"scenes": len(scenes), "fluid_particles": nfl,
+            "particles_min": int(min(counts)), "particles_max": int(max(counts)),
+            "precision": "f32 state, f64 number density", "steps": K,
+            "value": nfl * K / (ms_batch / 1e3), "ms_per_step": ms_batch / K,
+            "per_scene_loop_value": nfl * K / (ms_loop / 1e3), "per_scene_loop_ms_per_step": ms_loop / K,
+            "speedup_vs_per_scene_loop": ms_loop / ms_batch, "block_sizes": tuned,
+            "unit": "particle-updates/s"}
 
 
 def main():
@@ -348,6 +415,7 @@ def main():
     ap.add_argument("--precision", choices=["f32", "f64", "f32n64"], default="f32")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     world, rank, local = setup_dist()
     try:

@@ -272,6 +272,13 @@ int mps_get_counters(mps_handle* h, mps_counters* out);
 int mps_get_timing(mps_handle* h, int32_t kernel, double* total_ms, int64_t* launches,
                    int32_t reset);
 /*
+ * Autotuner: for each kernel group, time `trial_steps` steps at every candidate block size
+ * (32, 64, 96, 128 threads) with CUDA events and keep the fastest. The state is restored
+ * afterwards, so tuning changes no result (no kernel's arithmetic depends on its block
+ * size). chosen[MPS_K_COUNT] receives the block sizes (may be NULL).
+ */
+int mps_autotune(mps_handle* h, int32_t trial_steps, int32_t* chosen);
+/*
  * Integrals of scene `scene`: out[0..2] fluid centroid, out[3] kinetic energy per unit
  * mass (sum |v|^2 / 2), out[4] surge front (max x of fluid), out[5] alive fluid count.
  */

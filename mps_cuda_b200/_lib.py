@@ -101,6 +101,7 @@ SIGNATURES = {
     "mps_get_counters": (C.c_int, [C.c_void_p, C.POINTER(mps_counters)]),
     "mps_get_timing": (C.c_int, [C.c_void_p, C.c_int32, c_double_p, C.POINTER(C.c_int64),
                                  C.c_int32]),
+    "mps_autotune": (C.c_int, [C.c_void_p, C.c_int32, c_int32_p]),
     "mps_get_integrals": (C.c_int, [C.c_void_p, C.c_int32, c_double_p]),
     "mps_bucket_build_noalloc": (C.c_int, [C.POINTER(mps_params), C.c_int32, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

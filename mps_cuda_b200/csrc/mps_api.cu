@@ -156,6 +156,7 @@ int mps_set_option(mps_handle* h, int32_t opt, int32_t value) {
                 if (value != 0 && (value < 32 || value > 128 || value % 32))
                     throw ApiError(MPS_ERR_ARG, "block must be 0 or a multiple of 32 in [32, 128]");
                 s.block = value ? value : 128;
+                for (int g : {MPS_K_PASS_A, MPS_K_PASS_B, MPS_K_PASS_C, MPS_K_GEN}) s.blk[g] = s.block;
                 s.invalidate_graph();
                 break;
             case MPS_OPT_CELL_SKIP: s.skip_opt = value != 0; s.invalidate_graph(); break;
@@ -229,6 +230,11 @@ int mps_get_timing(mps_handle* h, int32_t kernel, double* total_ms, int64_t* lau
         s.timing(kernel, total_ms, &n, reset != 0);
         if (launches) *launches = n;
     });
+}
+
+int mps_autotune(mps_handle* h, int32_t trial_steps, int32_t* chosen) {
+    if (trial_steps <= 0) return fail(MPS_ERR_ARG, "trial_steps must be positive");
+    return guarded(h, [&](SolverBase& s) { s.autotune(trial_steps, chosen); });
 }
 
 int mps_get_integrals(mps_handle* h, int32_t scene, double out[6]) {

@@ -212,7 +212,9 @@ struct SolverBase {
     bool timing_on = false;
     double t_ms[MPS_K_COUNT] = {};
     long long t_n[MPS_K_COUNT] = {};
+    int blk[MPS_K_COUNT] = {128, 128, 128, 128, 256, 256};  // threads per block per group
     virtual void timing(int k, double* ms, long long* n, bool reset) = 0;
+    virtual void autotune(int trial, int32_t* chosen) = 0;
     virtual void step(int n) = 0;
     virtual void phase(int ph) = 0;
     virtual void get_state(int8_t*, void*, void*, void*, void*, void*) = 0;
@@ -571,11 +573,12 @@ template <class R, class RN> class Solver final : public SolverBase {
 
 
     template <bool D> void fused_body() {
-        const int gb = blocks(nF, block);
+        const int ba = blk[MPS_K_PASS_A], bb = blk[MPS_K_PASS_B], bc = blk[MPS_K_PASS_C],
+                  bg = blk[MPS_K_GEN];
         // pass A: VscTrm + UpPcl1
         {
             Scope t(this, MPS_K_PASS_A);
-            k_pass_a<R, RN, D><<<gb, block, 0, stream>>>(args(M1, mcs1));
+            k_pass_a<R, RN, D><<<blocks(nF, ba), ba, 0, stream>>>(args(M1, mcs1));
             KL();
         }
         // MkBkt on x* (kernel.cu:1917); the rebuild at kernel.cu:1921 would give the same lists
@@ -583,15 +586,15 @@ template <class R, class RN> class Solver final : public SolverBase {
         // pass B: ChkCol + MkPrs, then the second mirror generation at (x*, P)
         {
             Scope t(this, MPS_K_PASS_B);
-            k_pass_b<R, RN, D><<<gb, block, 0, stream>>>(args(M1, mcs1));
+            k_pass_b<R, RN, D><<<blocks(nF, bb), bb, 0, stream>>>(args(M1, mcs1));
             KL();
         }
         reset_raw();
         {
             Scope t(this, MPS_K_GEN);
             // the step's second generation: the one the reference's counters would show last
-            k_gen_cull<R, RN, D, false><<<gb, block, 0, stream>>>(args(M1, mcs1), S.pos, t_prs,
-                                                                  S.typ);
+            k_gen_cull<R, RN, D, false><<<blocks(nF, bg), bg, 0, stream>>>(args(M1, mcs1), S.pos,
+                                                                           t_prs, S.typ);
             KL();
             cull_raw();
         }
@@ -599,14 +602,14 @@ template <class R, class RN> class Solver final : public SolverBase {
         // pass C: PrsGrdTrm + UpPcl2, then the first mirror generation of the next step
         {
             Scope t(this, MPS_K_PASS_C);
-            k_pass_c<R, RN, D><<<gb, block, 0, stream>>>(args(M2, mcs2));
+            k_pass_c<R, RN, D><<<blocks(nF, bc), bc, 0, stream>>>(args(M2, mcs2));
             KL();
         }
         reset_raw();
         {
             Scope t(this, MPS_K_GEN);
-            k_gen_cull<R, RN, false, false><<<gb, block, 0, stream>>>(args(M2, mcs2), t_pos, t_prs,
-                                                                      t_typ);
+            k_gen_cull<R, RN, false, false><<<blocks(nF, bg), bg, 0, stream>>>(args(M2, mcs2), t_pos,
+                                                                               t_prs, t_typ);
             KL();
             cull_raw();
         }
@@ -634,6 +637,39 @@ template <class R, class RN> class Solver final : public SolverBase {
 
     void run_body() {
         if (diag_on) fused_body<true>(); else fused_body<false>();
+    }
+
+    void autotune(int trial, int32_t* chosen) override {
+        const int cand[] = {32, 64, 96, 128};
+        const int groups[] = {MPS_K_PASS_A, MPS_K_PASS_B, MPS_K_PASS_C, MPS_K_GEN};
+        double best[MPS_K_COUNT];
+        int bestb[MPS_K_COUNT];
+        for (int k = 0; k < MPS_K_COUNT; ++k) { best[k] = 1e300; bestb[k] = blk[k]; }
+        store_all();  // snapshot of the state in the id-order staging buffers
+        const long long steps0 = steps;
+        const bool timing0 = timing_on;
+        timing_on = true;
+        invalidate_graph();
+        timing(0, nullptr, nullptr, true);
+        for (int b : cand) {
+            for (int g : groups) blk[g] = b;
+            step(trial);
+            for (int g : groups) {
+                double ms = 0;
+                long long n = 0;
+                timing(g, &ms, &n, false);
+                if (n > 0 && ms / n < best[g]) { best[g] = ms / n; bestb[g] = b; }
+            }
+            timing(0, nullptr, nullptr, true);
+        }
+        for (int g : groups) blk[g] = bestb[g];
+        load_fluid(true);  // back to the snapshot: tuning leaves no trace in the results
+        steps = steps0;
+        timing_on = timing0;
+        invalidate_graph();
+        CK(cudaStreamSynchronize(stream));
+        if (chosen)
+            for (int k = 0; k < MPS_K_COUNT; ++k) chosen[k] = blk[k];
     }
 
     void invalidate_graph() override {

@@ -235,6 +235,12 @@ class MPSBatch:
             out[name] = (ms.value, n.value)
         return out
 
+    def autotune(self, trial_steps: int = 3) -> dict:
+        """Pick the fastest block size per kernel group (state restored afterwards)."""
+        out = (C.c_int32 * len(L.KERNEL_GROUPS))()
+        check(lib().mps_autotune(self._h, int(trial_steps), out), "mps_autotune")
+        return dict(zip(L.KERNEL_GROUPS, out[:]))
+
     def integrals(self, scene: int = 0) -> np.ndarray:
         out = (C.c_double * 6)()
         check(lib().mps_get_integrals(self._h, scene, out), "mps_get_integrals")

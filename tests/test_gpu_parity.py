@@ -171,3 +171,36 @@ def test_state_roundtrip_and_errors():
     g.step(3)
     o.step(3)
     _assert_same_state(g.state(), o.state())
+
+
+def test_autotune_changes_no_result():
+    g, o, _, _ = _pair("dambreak_l0.02_6k", F32, diag=False)
+    g.step(2)
+    chosen = g.autotune(2)
+    assert set(chosen["pass_a"] for _ in [0]) <= {32, 64, 96, 128}
+    assert g.counters()["steps"] == 2
+    g.step(3)
+    o.step(5)
+    _assert_same_state(g.state(), o.state())
+
+
+def test_batch_of_64_uneven_scenes_equals_separate_handles():
+    scenes = configs.batched_scenes()
+    parts = [dambreak(d) for d, _ in scenes]
+    params = [dambreak_params(d, dt=dt, precision=F32_N64) for d, dt in scenes]
+    counts = [p["typ"].shape[0] for p in parts]
+    cat = lambda k: np.concatenate([p[k] for p in parts], axis=-1).astype(
+        np.float32 if k != "typ" else np.int8)
+    b = MPSBatch(params, cat("typ"), cat("pos"), cat("vel"), cat("nrm"), counts=counts)
+    b.set_option(L.OPT_GRAPH, 1)
+    b.step(4)
+    st = b.state()
+    off = 0
+    for pp, pt, n in zip(params, parts, counts):
+        h = MPS(pp, pt["typ"], pt["pos"].astype(np.float32), pt["vel"].astype(np.float32),
+                pt["nrm"].astype(np.float32))
+        h.step(4)
+        sub = {k: v[..., off:off + n] for k, v in st.items()}
+        _assert_same_state(sub, h.state())
+        h.close()
+        off += n

@@ -17,13 +17,16 @@ ours      : libmps_b200.so. `value` = device time of K steps (CUDA events on the
             `cpu_baseline` = the CPU oracle (OpenMP restatement of the reference's
             per-particle loops) on a bounded sample of the same workload, rank 0 only.
 reference : the reference's per-particle loops as that OpenMP CPU restatement (the
-            reference itself has no CPU implementation), all host threads, rank 0 only.
+            reference itself has no CPU implementation), all host threads, rank 0 only;
+            `reference_cuda` adds the reference's own CUDA kernels (built for sm_100a from
+            its sources) on the same workload and GPU, where that build is present.
 Under torchrun (N > 1) each rank advances its own copy of the workload on its own GPU
 (replicas: the step has no exchange between scenes), so `value` counts all ranks' updates.
 """
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import os
 import statistics
@@ -190,12 +193,65 @@ def cpu_oracle_rate(p, typ, pos, vel, nrm, budget_s: float, max_steps: int, warm
     return nf * k / el, k, threads, el
 
 
+@contextlib.contextmanager
+def _c_stdout_silenced():
+    """Send what C code writes to file descriptor 1 to /dev/null for the duration."""
+    import ctypes
+    sys.stdout.flush()
+    libc = ctypes.CDLL(None)
+    saved = os.dup(1)
+    null = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(null, 1)
+    try:
+        yield
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(null)
+
+
+def reference_cuda_rate(p, typ, pos, vel, nrm, steps: int, warmup: int):
+    """The reference's own CUDA kernels on the same workload, as a same-box reference point.
+
+    oracle/_ref/libref_mps_{f32,f64}.so is `class MPS` built for sm_100a from the reference
+    sources (oracle/ref_build.sh); its step is ClcMPS's loop body (kernel.cu:1904-1935),
+    default stream, a device synchronise after every kernel as the reference does. Timed by
+    wall clock around that synchronised loop, L2 not flushed. None where the library or a GPU
+    is missing, or for the mixed precision the reference does not have.
+    """
+    from mps_cuda_b200 import F32, F64
+    if p.precision not in (F32, F64):
+        return None
+    from oracle import refbind
+    prec = 1 if p.precision == F64 else 0
+    if not refbind.available(prec):
+        return None
+    import torch
+    if not torch.cuda.is_available():
+        return None
+    torch.cuda.set_device(0)
+    with _c_stdout_silenced():  # SetPara prints its constants; keep stdout to the JSON line
+        ref = refbind.Reference(p, typ, pos, vel, nrm)
+        ref.step(max(warmup, 1))
+        t0 = time.perf_counter()
+        ref.step(steps)
+        el = time.perf_counter() - t0
+    nf = int((typ == 0).sum())
+    return {"value": nf * steps / el, "unit": "particle-updates/s", "ms_per_step": 1e3 * el / steps,
+            "steps": steps, "warmup": max(warmup, 1),
+            "implementation": "the reference's class MPS kernels built for sm_100a, its own "
+                              "synchronised step loop, timed by wall clock"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
     p, typ, pos, vel, nrm = build_scene(args.workload, args.precision)
     rate, k, threads, el = cpu_oracle_rate(p, typ, pos, vel, nrm, budget_s=150.0,
                                            max_steps=args.steps, warmup=min(args.warmup, 2))
+    ref_cuda = reference_cuda_rate(p, typ, pos, vel, nrm, steps=args.steps,
+                                   warmup=max(args.warmup, 3))
     sample = (f"{k} full steps of the {args.workload} workload ({int((typ == 0).sum())} fluid "
               f"particles) after {min(args.warmup, 2)} warm-up step(s), {threads} OpenMP threads")
     line = {"metric": METRIC, "value": rate, "unit": "particle-updates/s", "impl": "reference",
@@ -208,7 +264,8 @@ def run_reference(args, world, rank):
             "cpu_baseline": {"value": rate, "unit": "particle-updates/s", "cores": threads,
                              "kind": "port", "sample": sample},
             "e2e": {"value": rate, "unit": "particle-updates/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "reference_cuda": ref_cuda}
     print(json.dumps(line), flush=True)
 
 
@@ -318,7 +375,7 @@ def run_ours(args, world, rank, local):
     clk.__exit__(None, None, None)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, k, threads, el = cpu_oracle_rate(p, typ, pos, vel, nrm, budget_s=20.0, max_steps=10)
+        rate, k, threads, el = cpu_oracle_rate(p, typ, pos, vel, nrm, budget_s=20.0, max_steps=200)
         cpu = {"value": rate, "unit": "particle-updates/s", "cores": threads, "kind": "port",
                "sample": f"{k} steps of the same workload after 1 warm-up step ({el:.1f} s)"}
 

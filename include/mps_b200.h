@@ -279,6 +279,30 @@ int mps_get_timing(mps_handle* h, int32_t kernel, double* total_ms, int64_t* lau
  */
 int mps_autotune(mps_handle* h, int32_t trial_steps, int32_t* chosen);
 /*
+ * Adjoint of a rollout. The reference has no derivative of its step; these two calls add
+ * one behind the same state layout.
+ *
+ * mps_adjoint_record advances the handle `nsteps` steps (as mps_step) and keeps the state
+ * every `checkpoint_every` steps on the device. Single-scene handles only.
+ *
+ * mps_adjoint_backward takes the adjoint of a scalar loss with respect to the final
+ * positions and velocities (SoA x[n], y[n], z[n], doubles, particle-id order; NULL = zero)
+ * and returns its gradients with respect to the positions and velocities at the start of
+ * the rollout (same layout; NULL = not wanted) and to the kinematic viscosity knm_vsc
+ * (*grad_nu, host memory; NULL = not wanted). Array pointers may be host or device
+ * memory. Entries of wall particles are zero. It recomputes each segment from its
+ * checkpoint, holding the recorded step's discrete choices fixed (neighbour lists, mirror
+ * sets, collision branches, the pressure-minimum neighbour, clamps and deletions), and
+ * leaves the handle at the final state of the rollout. It can be called again on the same
+ * recording. MPS_ERR_OVERFLOW if a neighbour list of the rollout exceeded its capacity.
+ * Device memory per step of one segment: two neighbour lists of 160 int32 per fluid
+ * particle, about 200 bytes of state per fluid particle, and two mirror generations of
+ * 10 slots x 68 bytes per fluid particle.
+ */
+int mps_adjoint_record(mps_handle* h, int32_t nsteps, int32_t checkpoint_every);
+int mps_adjoint_backward(mps_handle* h, const double* lam_pos, const double* lam_vel,
+                         double* grad_pos0, double* grad_vel0, double* grad_nu);
+/*
  * Integrals of scene `scene`: out[0..2] fluid centroid, out[3] kinetic energy per unit
  * mass (sum |v|^2 / 2), out[4] surge front (max x of fluid), out[5] alive fluid count.
  */

@@ -103,6 +103,9 @@ SIGNATURES = {
                                  C.c_int32]),
     "mps_autotune": (C.c_int, [C.c_void_p, C.c_int32, c_int32_p]),
     "mps_get_integrals": (C.c_int, [C.c_void_p, C.c_int32, c_double_p]),
+    "mps_adjoint_record": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    "mps_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, c_double_p]),
     "mps_bucket_build_noalloc": (C.c_int, [C.POINTER(mps_params), C.c_int32, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p]),

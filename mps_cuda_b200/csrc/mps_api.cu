@@ -232,6 +232,19 @@ int mps_get_timing(mps_handle* h, int32_t kernel, double* total_ms, int64_t* lau
     });
 }
 
+int mps_adjoint_record(mps_handle* h, int32_t nsteps, int32_t checkpoint_every) {
+    if (nsteps <= 0 || checkpoint_every <= 0)
+        return fail(MPS_ERR_ARG, "nsteps and checkpoint_every must be positive");
+    return guarded(h, [&](SolverBase& s) { s.adjoint_record(nsteps, checkpoint_every); });
+}
+
+int mps_adjoint_backward(mps_handle* h, const double* lam_pos, const double* lam_vel,
+                         double* grad_pos0, double* grad_vel0, double* grad_nu) {
+    return guarded(h, [&](SolverBase& s) {
+        s.adjoint_backward(lam_pos, lam_vel, grad_pos0, grad_vel0, grad_nu);
+    });
+}
+
 int mps_autotune(mps_handle* h, int32_t trial_steps, int32_t* chosen) {
     if (trial_steps <= 0) return fail(MPS_ERR_ARG, "trial_steps must be positive");
     return guarded(h, [&](SolverBase& s) { s.autotune(trial_steps, chosen); });

@@ -149,6 +149,9 @@ template <class R> struct MirrorSink {
     V4<R>* pos;
     int* slot;
     int cap;
+    // recorded rollouts only: per raw mirror n * sqrt(2 / |n|) of its reflection plane's
+    // normal n, so that d(mirror)/d(owner) = I - nrm nrm^T
+    V4<R>* nrm;
 };
 
 // ---- VscTrm sum (kernel.cu:1037-1107) ----------------------------------------------------
@@ -196,6 +199,18 @@ __device__ __forceinline__ void visc_sum(const SceneDev<R, RN>& sc, const RowCtx
         }
     });
     visc_sum_mirrors(sc, c, x, y, z, ux, uy, uz, m, B, sx, sy, sz, cm);
+}
+
+// out-of-line copy for the rare slot whose neighbour list overflowed its capacity
+template <class R, class RN>
+__device__ __noinline__ void visc_sum_outline(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
+                                              R x, R y, R z, R ux, R uy, R uz,
+                                              const int* __restrict__ cs,
+                                              const V4<R>* __restrict__ pos,
+                                              const V4<R>* __restrict__ vel,
+                                              const MirrorView<R>& m, R B, R& sx, R& sy, R& sz,
+                                              int& cf, int& cm) {
+    visc_sum(sc, c, s, x, y, z, ux, uy, uz, cs, pos, vel, m, B, sx, sy, sz, cf, cm);
 }
 
 // ---- ChkPcl (kernel.cu:481-513); returns false when the particle is deleted --------------
@@ -305,6 +320,21 @@ __device__ __forceinline__ void col_dens_sum(const SceneDev<R, RN>& sc, const Ro
     });
     col_dens_walls_mirrors<R, RN, COL, DENS>(sc, c, x, y, z, ux, uy, uz, wl, m, skip, wx, wy, wz,
                                              ni, cnt);
+}
+
+// out-of-line copy for the rare slot whose neighbour list overflowed its capacity: keeps
+// the scan's code out of the list-walking kernel's instruction stream
+template <class R, class RN, bool COL, bool DENS>
+__device__ __noinline__ void col_dens_sum_outline(const SceneDev<R, RN>& sc, const RowCtx<R>& c,
+                                                  int s, R x, R y, R z, R ux, R uy, R uz,
+                                                  const int* __restrict__ cs,
+                                                  const V4<R>* __restrict__ pos,
+                                                  const V4<R>* __restrict__ vel,
+                                                  const WallView<R>& wl, const MirrorView<R>& m,
+                                                  bool skip, R& wx, R& wy, R& wz, RN& ni,
+                                                  int* cnt) {
+    col_dens_sum<R, RN, COL, DENS>(sc, c, s, x, y, z, ux, uy, uz, cs, pos, vel, wl, m, skip, wx,
+                                   wy, wz, ni, cnt);
 }
 
 // explicit equation of state with clamps, kernel.cu:1388-1406
@@ -426,7 +456,7 @@ __device__ __forceinline__ bool cull_keep(const SceneDev<R, RN>& sc, R mx, R my,
 // ---- GenMRR_nonslip for one fluid particle (kernel.cu:726-891) ---------------------------
 // Appends the mirrors (culled on the spot when CULL) to `out`; returns the number of walls
 // inside r (diagnostic).
-template <class R, class RN, bool CULL>
+template <class R, class RN, bool CULL, bool TAPE = false>
 __device__ __forceinline__ int gen_mirrors(const SceneDev<R, RN>& sc, const RowCtx<R>& c, R x,
                                            R y, R z, R P, int slot_base, const WallView<R>& wl,
                                            bool skip, const MirrorSink<R>& out,
@@ -461,12 +491,16 @@ __device__ __forceinline__ int gen_mirrors(const SceneDev<R, RN>& sc, const RowC
         }
     });
     if (nreg == 0) return nwall;
-    auto emit = [&](R mx, R my, R mz, int slot) {
+    auto emit = [&](R mx, R my, R mz, int slot, R nx, R ny, R nz, R nlen) {
         if (CULL && !cull_keep(sc, mx, my, mz, wl, skip, &cnt->err_cell)) return;
         int idx = atomicAdd(&cnt->mirror_raw, 1);
         if (idx < out.cap) {
             out.pos[idx] = V4<R>{mx, my, mz, P};
             out.slot[idx] = slot;
+            if (TAPE) {
+                const R c = sqrtR(R(2) / nlen);
+                out.nrm[idx] = V4<R>{nx * c, ny * c, nz * c, R(0)};
+            }
         } else {
             atomicAdd(&cnt->err_capacity, 1);
         }
@@ -477,10 +511,11 @@ __device__ __forceinline__ int gen_mirrors(const SceneDev<R, RN>& sc, const RowC
         R pwx = x - q.x, pwy = y - q.y, pwz = z - q.z;
         R pw = dot3(pwx, pwy, pwz, rn[k][0], rn[k][1], rn[k][2]);
         if (pw < R(0)) continue;
-        R dist = pw / sqrtR(dot3(rn[k][0], rn[k][1], rn[k][2], rn[k][0], rn[k][1], rn[k][2]));
+        R nlen = sqrtR(dot3(rn[k][0], rn[k][1], rn[k][2], rn[k][0], rn[k][1], rn[k][2]));
+        R dist = pw / nlen;
         R t2 = R(2) * dist;
         emit(fmaR(-t2, rn[k][0], q.x + pwx), fmaR(-t2, rn[k][1], q.y + pwy),
-             fmaR(-t2, rn[k][2], q.z + pwz), slot_base + k);
+             fmaR(-t2, rn[k][2], q.z + pwz), slot_base + k, rn[k][0], rn[k][1], rn[k][2], nlen);
     }
     // corner mirror through the last edge wall (kernel.cu:841-887)
     if (nedge >= 2) {
@@ -494,13 +529,14 @@ __device__ __forceinline__ int gen_mirrors(const SceneDev<R, RN>& sc, const RowC
         sx /= as; sy /= as; sz /= as;
         R pw = dot3(pwx, pwy, pwz, sx, sy, sz);
         if (pw >= R(0)) {
-            R dist = pw / sqrtR(dot3(sx, sy, sz, sx, sy, sz));
+            R slen = sqrtR(dot3(sx, sy, sz, sx, sy, sz));
+            R dist = pw / slen;
             if (nreg >= kNumMRR) {
                 atomicAdd(&cnt->err_mirror_slot, 1);
             } else {
                 R t2 = R(2) * dist;
                 emit(fmaR(-t2, sx, q.x + pwx), fmaR(-t2, sy, q.y + pwy),
-                     fmaR(-t2, sz, q.z + pwz), slot_base + nreg);
+                     fmaR(-t2, sz, q.z + pwz), slot_base + nreg, sx, sy, sz, slen);
             }
         }
     }

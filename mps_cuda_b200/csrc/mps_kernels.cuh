@@ -160,6 +160,17 @@ template <class R> struct MirrorGather {
     }
 };
 
+// MirrorGather that also carries the recorded reflection normals
+template <class R> struct MirrorGatherN {
+    const V4<R>* pos; const int* slot; const V4<R>* nrm;
+    V4<R>* dpos; int* dslot; V4<R>* dnrm;
+    __device__ __forceinline__ void operator()(int t, int d) const {
+        dpos[d] = pos[t];
+        dslot[d] = slot[t];
+        dnrm[d] = nrm[t];
+    }
+};
+
 template <class R> struct WallGather {
     const V4<R>* pos; const V4<R>* nrm; const V4<R>* vel; const int* wid; const int8_t* typ;
     V4<R>* dpos; V4<R>* dnrm; V4<R>* dvel; int* dwid; int8_t* dtyp;
@@ -271,6 +282,9 @@ template <class R, class RN> struct PassArgs {
     int* nbcnt;
     int nbK;
     const int8_t* near_wall;  // per bucket: a wall lies in the 27 buckets around it
+    // recorded rollouts only: per slot the velocity before ChkPcl's clamp, w = slot state
+    // (kTapeOk, kTapeClamped, kTapeDeleted, kTapeDead)
+    V4<R>* tape_pre;
 };
 
 // near_wall flag of every bucket of every scene (walls are static: computed once)
@@ -336,8 +350,24 @@ __device__ __forceinline__ int build_list(const PassArgs<R, RN>& a, const SceneD
     return cnt;
 }
 
-// pass A: VscTrm (kernel.cu:1013-1119) + UpPcl1/ChkPcl (kernel.cu:1138-1149, 481-513)
-template <class R, class RN, bool DIAG>
+// state of a slot in a recorded step, kept in the w component of the pre-clamp velocity
+constexpr int kTapeOk = 0, kTapeClamped = 1, kTapeDeleted = 2, kTapeDead = 3;
+
+// the velocity a kick produced before ChkPcl (kernel.cu:481-513) and what ChkPcl will do
+// with it: delete the particle (position outside the box) or clamp |u| to umax
+template <class R, class RN>
+__device__ __forceinline__ void tape_record(const PassArgs<R, RN>& a, const SceneDev<R, RN>& sc,
+                                            int s, R x, R y, R z, R ux, R uy, R uz) {
+    int st = kTapeDeleted;
+    if (x < sc.hi[0] && x > sc.lo[0] && y < sc.hi[1] && y > sc.lo[1] && z < sc.hi[2] &&
+        z > sc.lo[2])
+        st = sqrtR(dot3(ux, uy, uz, ux, uy, uz)) > sc.umax ? kTapeClamped : kTapeOk;
+    a.tape_pre[s] = V4<R>{ux, uy, uz, R(st)};
+}
+
+// pass A: VscTrm (kernel.cu:1013-1119) + UpPcl1/ChkPcl (kernel.cu:1138-1149, 481-513).
+// TAPE (recorded rollouts): also keeps the list length and the velocity before the clamp.
+template <class R, class RN, bool DIAG, bool TAPE = false>
 __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
@@ -346,6 +376,10 @@ __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
         a.tpos[s] = a.pos[s];
         a.tvel[s] = a.vel[s];
         a.ttyp[s] = a.typ[s];
+        if (TAPE) {
+            a.tape_pre[s] = V4<R>{R(0), R(0), R(0), R(kTapeDead)};
+            a.nbcnt[s] = 0;
+        }
         return;
     }
     const int pid = a.pid[s];
@@ -357,6 +391,7 @@ __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
     R sx = 0, sy = 0, sz = 0;
     int cf = 0, cm = 0;
     const int n = build_list(a, sc, c, s, p.x, p.y, p.z, sc.r_le, MPS_INF_SKIP(a, sc.skip_r));
+    if (TAPE) a.nbcnt[s] = n;
     if (n <= a.nbK) {
         const int* __restrict__ nb = a.nb + s;
         const V4<R>* __restrict__ pos = a.pos;
@@ -387,12 +422,13 @@ __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
         visc_sum_mirrors(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.m, MPS_INF_SKIP(a, sc.skip_r), sx, sy,
                          sz, cm);
     } else {
-        visc_sum(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.cs, a.pos, a.vel, a.m,
-                 MPS_INF_SKIP(a, sc.skip_r), sx, sy, sz, cf, cm);
+        visc_sum_outline(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.cs, a.pos, a.vel, a.m,
+                         MPS_INF_SKIP(a, sc.skip_r), sx, sy, sz, cf, cm);
     }
     R ax = fmaR(sc.kn, sx, sc.g[0]), ay = fmaR(sc.kn, sy, sc.g[1]), az = fmaR(sc.kn, sz, sc.g[2]);
     R ux = fmaR(ax, sc.dt, v.x), uy = fmaR(ay, sc.dt, v.y), uz = fmaR(az, sc.dt, v.z);
     R x = fmaR(ux, sc.dt, p.x), y = fmaR(uy, sc.dt, p.y), z = fmaR(uz, sc.dt, p.z);
+    if (TAPE) tape_record(a, sc, s, x, y, z, ux, uy, uz);
     bool alive = chkpcl(sc, x, y, z, ux, uy, uz);
     if (!alive) {
         x = y = z = ux = uy = uz = R(0);
@@ -468,8 +504,12 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
         col_dens_walls_mirrors<R, RN, true, true>(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.wl, a.m,
                                                   a.skip != 0, wx, wy, wz, ni, cnt5);
     } else {
-        col_dens_sum<R, RN, true, true>(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.cs, a.pos,
-                                        a.vel, a.wl, a.m, a.skip != 0, wx, wy, wz, ni, cnt5);
+        int t5[5] = {0, 0, 0, 0, 0};  // a separate array keeps cnt5 in registers
+        col_dens_sum_outline<R, RN, true, true>(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.cs,
+                                                a.pos, a.vel, a.wl, a.m, a.skip != 0, wx, wy, wz,
+                                                ni, t5);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) cnt5[k] = t5[k];
     }
     R P = eos(sc, ni);
     a.tvel[s] = V4<R>{wx, wy, wz, R(0)};
@@ -486,8 +526,8 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
 }
 
 // pass C: PrsGrdTrm (kernel.cu:1651-1794) + UpPcl2/ChkPcl (kernel.cu:1815-1829), walking
-// the neighbour lists pass B left
-template <class R, class RN, bool DIAG>
+// the neighbour lists pass B left. TAPE: also keeps the velocity before the clamp.
+template <class R, class RN, bool DIAG, bool TAPE = false>
 __global__ void __launch_bounds__(128) k_pass_c(PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
@@ -495,6 +535,7 @@ __global__ void __launch_bounds__(128) k_pass_c(PassArgs<R, RN> a) {
     if (s >= nalive) {
         a.tpos[s] = a.pos[s];
         a.ttyp[s] = a.typ[s];
+        if (TAPE) a.tape_pre[s] = V4<R>{R(0), R(0), R(0), R(kTapeDead)};
         return;
     }
     const int pid = a.pid[s];
@@ -574,6 +615,7 @@ __global__ void __launch_bounds__(128) k_pass_c(PassArgs<R, RN> a) {
     R x = fmaR(ax * sc.dt, sc.dt, p.x), y = fmaR(ay * sc.dt, sc.dt, p.y),
       z = fmaR(az * sc.dt, sc.dt, p.z);
     a.pav[s] = a.pav[s] + pi;
+    if (TAPE) tape_record(a, sc, s, x, y, z, ux, uy, uz);
     bool alive = chkpcl(sc, x, y, z, ux, uy, uz);
     if (!alive) {
         x = y = z = ux = uy = uz = R(0);
@@ -593,7 +635,7 @@ __global__ void __launch_bounds__(128) k_pass_c(PassArgs<R, RN> a) {
 // of a step (x*, P after pass B) and the first generation of the next one (x^{n+1}, P after
 // pass C). Near-wall particles are a thin layer, so this runs as a light kernel of its own
 // instead of stretching the neighbour passes.
-template <class R, class RN, bool DIAG, bool CULL>
+template <class R, class RN, bool DIAG, bool CULL, bool TAPE = false>
 __global__ void __launch_bounds__(128) k_gen_cull(PassArgs<R, RN> a, const V4<R>* gpos,
                                                   const R* gprs, const int8_t* gtyp) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -609,8 +651,8 @@ __global__ void __launch_bounds__(128) k_gen_cull(PassArgs<R, RN> a, const V4<R>
         return;
     }
     RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
-    int nw = gen_mirrors<R, RN, CULL>(sc, c, p.x, p.y, p.z, gprs[s], pid * kNumMRR, a.wl,
-                                      a.skip != 0, a.out, a.cnt);
+    int nw = gen_mirrors<R, RN, CULL, TAPE>(sc, c, p.x, p.y, p.z, gprs[s], pid * kNumMRR, a.wl,
+                                            a.skip != 0, a.out, a.cnt);
     if (DIAG) a.diag[size_t(pid) * kDiagCols + DG_GEN_W] = nw;
 }
 

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/mps_b200.h"
+#include "mps_adjoint.cuh"
 #include "mps_kernels.cuh"
 
 namespace mps {
@@ -226,6 +227,9 @@ struct SolverBase {
     virtual void get_counters(mps_counters*) = 0;
     virtual void integrals(int scene, double out[6]) = 0;
     virtual void invalidate_graph() = 0;
+    virtual void adjoint_record(int nsteps, int every) = 0;
+    virtual void adjoint_backward(const double* lam_pos, const double* lam_vel, double* g_pos,
+                                  double* g_vel, double* g_nu) = 0;
 };
 
 template <class R, class RN> class Solver final : public SolverBase {
@@ -556,10 +560,11 @@ template <class R, class RN> class Solver final : public SolverBase {
         a.tpos = t_pos; a.tvel = t_vel; a.tprs = t_prs; a.ttyp = t_typ;
         a.wl = wall_view();
         a.m = MirrorView<R>{mcs, m.pos, m.slot};
-        a.out = MirrorSink<R>{U.pos, U.slot, cap};
+        a.out = MirrorSink<R>{U.pos, U.slot, cap, nullptr};
         a.cnt = cnt; a.diag = diag; a.ndens = ndens;
         a.nb = nb; a.nbcnt = nbcnt; a.nbK = nbK;
         a.near_wall = near_wall;
+        a.tape_pre = nullptr;
         return a;
     }
 
@@ -929,6 +934,264 @@ template <class R, class RN> class Solver final : public SolverBase {
         o->err_cell_range = c.err_cell;
         o->err_nan = c.err_nan;
         o->kernel_launches = launches;
+    }
+
+    // ---- adjoint of a recorded rollout -------------------------------------------------
+    // A rollout of n steps keeps the state every k steps (particle-id order, as the staging
+    // buffers hold it). The backward sweep walks the segments last to first: it restores a
+    // segment's first state, replays the segment's steps with the recording kernels (which
+    // keep the neighbour lists, mirror generations and pre-clamp velocities of each step)
+    // and runs the step adjoints in reverse over what they kept. The replay repeats the
+    // original steps exactly: the bucket order and every sum depend on the state only.
+    struct Ckpt {
+        R* pos; R* vel; R* prs; R* pav; int8_t* typ;
+    };
+    struct AdjState {
+        DevArena ar;
+        int nsteps = 0, every = 0, nck = 0;
+        long long steps_end = 0;
+        std::vector<Ckpt> ck;  // nck segment starts + the final state
+        std::vector<TapeStep<R>> tape;
+        V4<R>* unrm = nullptr;
+        V4<double> *lx, *lv, *lx_acc, *lG, *lvv, *lxs, *lx_at, *lxs_pid, *lu_pid, *la, *lxa, *lva;
+        double *lP, *lP_at, *lkn, *stage;
+        R* pmin;
+        int *am, *inv2, *err;
+    };
+    std::unique_ptr<AdjState> adj;
+
+    void snapshot(const Ckpt& c) {
+        store_all();
+        const size_t n3 = 3 * size_t(nT) * sizeof(R), n1 = size_t(nT) * sizeof(R);
+        CK(cudaMemcpyAsync(c.pos, io.pos, n3, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(c.vel, io.vel, n3, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(c.prs, io.prs, n1, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(c.pav, io.pav, n1, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(c.typ, io.typ, nT, cudaMemcpyDeviceToDevice, stream));
+    }
+
+    void restore(const Ckpt& c) {
+        const size_t n3 = 3 * size_t(nT) * sizeof(R), n1 = size_t(nT) * sizeof(R);
+        CK(cudaMemcpyAsync(io.pos, c.pos, n3, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(io.vel, c.vel, n3, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(io.prs, c.prs, n1, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(io.pav, c.pav, n1, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(io.typ, c.typ, nT, cudaMemcpyDeviceToDevice, stream));
+        load_fluid(false);
+    }
+
+    void adj_alloc(int nck, int every) {
+        adj.reset();
+        auto st = std::make_unique<AdjState>();
+        DevArena& a = st->ar;
+        const size_t F = std::max(nF, 1), T = std::max(nT, 1), Cm = size_t(cap), Lc = L() + 1;
+        for (int c = 0; c <= nck; ++c)
+            st->ck.push_back(Ckpt{a.template get<R>(3 * T), a.template get<R>(3 * T),
+                                  a.template get<R>(T), a.template get<R>(T),
+                                  a.template get<int8_t>(T)});
+        for (int k = 0; k < every; ++k) {
+            TapeStep<R> t;
+            t.pid1 = a.template get<int>(F); t.x1 = a.template get<V4<R>>(F);
+            t.v1 = a.template get<V4<R>>(F); t.up1 = a.template get<V4<R>>(F);
+            t.nA = a.template get<int>(F); t.nbA = a.template get<int>(size_t(nbK) * F);
+            t.m1pos = a.template get<V4<R>>(Cm); t.m1slot = a.template get<int>(Cm);
+            t.m1nrm = a.template get<V4<R>>(Cm); t.mcs1 = a.template get<int>(Lc);
+            t.pid2 = a.template get<int>(F); t.x2 = a.template get<V4<R>>(F);
+            t.u2 = a.template get<V4<R>>(F); t.vv2 = a.template get<V4<R>>(F);
+            t.P2 = a.template get<R>(F); t.vp2 = a.template get<V4<R>>(F);
+            t.nB = a.template get<int>(F); t.nbB = a.template get<int>(size_t(nbK) * F);
+            t.m2pos = a.template get<V4<R>>(Cm); t.m2slot = a.template get<int>(Cm);
+            t.m2nrm = a.template get<V4<R>>(Cm); t.mcs2 = a.template get<int>(Lc);
+            st->tape.push_back(t);
+        }
+        st->unrm = a.template get<V4<R>>(Cm);
+        for (V4<double>** p : {&st->lx, &st->lv, &st->lx_acc, &st->lxs_pid, &st->lu_pid})
+            *p = a.template get<V4<double>>(T);
+        for (V4<double>** p : {&st->lG, &st->lvv, &st->lxs, &st->lx_at, &st->la, &st->lxa, &st->lva})
+            *p = a.template get<V4<double>>(F);
+        st->lP = a.template get<double>(F);
+        st->lP_at = a.template get<double>(F);
+        st->lkn = a.template get<double>(1);
+        st->stage = a.template get<double>(3 * T);
+        st->pmin = a.template get<R>(F);
+        st->am = a.template get<int>(F);
+        st->inv2 = a.template get<int>(T);
+        st->err = a.template get<int>(1);
+        st->nck = nck;
+        st->every = every;
+        adj = std::move(st);
+    }
+
+    void adjoint_record(int nsteps, int every) override {
+        if (nscene != 1)
+            throw ApiError(MPS_ERR_UNSUPPORTED, "the adjoint runs on single-scene handles");
+        if (nsteps <= 0 || every <= 0)
+            throw ApiError(MPS_ERR_ARG, "nsteps and checkpoint_every must be positive");
+        every = std::min(every, nsteps);
+        const int nck = (nsteps + every - 1) / every;
+        if (!adj || adj->nck != nck || adj->every != every) adj_alloc(nck, every);
+        adj->nsteps = 0;
+        for (int c = 0; c < nck; ++c) {
+            snapshot(adj->ck[c]);
+            step(std::min(every, nsteps - c * every));
+        }
+        snapshot(adj->ck[nck]);
+        adj->nsteps = nsteps;
+        adj->steps_end = steps;
+        CK(cudaStreamSynchronize(stream));
+    }
+
+    // mirrors from the raw list into tape buffers, normals included
+    void bin_mirrors_n(V4<R>* dpos, int* dslot, V4<R>* dnrm, int* dcs) {
+        MirrorKeySrc<R, RN> ks{d_sc, nscene, dead(), U.pos, U.slot};
+        MirrorGatherN<R> g{U.pos, U.slot, adj->unrm, dpos, dslot, dnrm};
+        bin(ks, g, &cnt->mirror_raw, cap, dcs);
+    }
+
+    PassArgs<R, RN> tape_args(const V4<R>* mpos, const int* mslot, const int* mcs, int* nbl,
+                              int* nbc, V4<R>* pre) {
+        PassArgs<R, RN> a = args(M1, mcs1);
+        a.m = MirrorView<R>{mcs, mpos, mslot};
+        a.nb = nbl;
+        a.nbcnt = nbc;
+        a.tape_pre = pre;
+        a.out.nrm = adj->unrm;
+        return a;
+    }
+
+    // the first mirror generation of a replayed segment, as prepare_fused makes it
+    void tape_prepare(const TapeStep<R>& t) {
+        mkbkt(false);
+        reset_raw();
+        PassArgs<R, RN> a = tape_args(M1.pos, M1.slot, mcs1, nb, nbcnt, nullptr);
+        k_gen_cull<R, RN, false, false, true><<<blocks(nF, block), block, 0, stream>>>(
+            a, S.pos, S.prs, S.typ);
+        KL();
+        cull_raw();
+        bin_mirrors_n(t.m1pos, t.m1slot, t.m1nrm, t.mcs1);
+    }
+
+    // fused_body with the recording kernels; `next` receives the next step's mirrors
+    void tape_body(const TapeStep<R>& t, const TapeStep<R>* next) {
+        const int ba = blk[MPS_K_PASS_A], bb = blk[MPS_K_PASS_B], bc = blk[MPS_K_PASS_C],
+                  bg = blk[MPS_K_GEN];
+        const size_t F = size_t(nF);
+        auto cp = [&](void* d, const void* s, size_t bytes) {
+            CK(cudaMemcpyAsync(d, s, bytes, cudaMemcpyDeviceToDevice, stream));
+        };
+        cp(t.pid1, S.pid, sizeof(int) * F);
+        cp(t.x1, S.pos, sizeof(V4<R>) * F);
+        cp(t.v1, S.vel, sizeof(V4<R>) * F);
+        PassArgs<R, RN> a = tape_args(t.m1pos, t.m1slot, t.mcs1, t.nbA, t.nA, t.up1);
+        k_pass_a<R, RN, false, true><<<blocks(nF, ba), ba, 0, stream>>>(a);
+        KL();
+        bin_fluid(t_pos, t_vel, nullptr, S.prs, S.pav, S.pid, t_typ);
+        a = tape_args(t.m1pos, t.m1slot, t.mcs1, t.nbB, t.nB, nullptr);
+        k_pass_b<R, RN, false><<<blocks(nF, bb), bb, 0, stream>>>(a);
+        KL();
+        cp(t.pid2, S.pid, sizeof(int) * F);
+        cp(t.x2, S.pos, sizeof(V4<R>) * F);
+        cp(t.u2, S.vel, sizeof(V4<R>) * F);
+        cp(t.vv2, t_vel, sizeof(V4<R>) * F);
+        cp(t.P2, t_prs, sizeof(R) * F);
+        reset_raw();
+        k_gen_cull<R, RN, false, false, true><<<blocks(nF, bg), bg, 0, stream>>>(a, S.pos, t_prs,
+                                                                                S.typ);
+        KL();
+        cull_raw();
+        bin_mirrors_n(t.m2pos, t.m2slot, t.m2nrm, t.mcs2);
+        a = tape_args(t.m2pos, t.m2slot, t.mcs2, t.nbB, t.nB, t.vp2);
+        k_pass_c<R, RN, false, true><<<blocks(nF, bc), bc, 0, stream>>>(a);
+        KL();
+        reset_raw();
+        k_gen_cull<R, RN, false, false, true><<<blocks(nF, bg), bg, 0, stream>>>(a, t_pos, t_prs,
+                                                                                t_typ);
+        KL();
+        cull_raw();
+        bin_fluid(t_pos, t_vel, nullptr, t_prs, S.pav, S.pid, t_typ);
+        if (next) bin_mirrors_n(next->m1pos, next->m1slot, next->m1nrm, next->mcs1);
+        else bin_mirrors(M1, mcs1);
+    }
+
+    void back_step(const TapeStep<R>& t) {
+        AdjState& s = *adj;
+        AdjArgs<R, RN> A;
+        A.sc = d_sc; A.nF = nF; A.nbK = nbK; A.t = t; A.wl = wall_view();
+        A.lx = s.lx; A.lv = s.lv; A.lx_acc = s.lx_acc;
+        A.lG = s.lG; A.lvv = s.lvv; A.lxs = s.lxs; A.lx_at = s.lx_at;
+        A.lP = s.lP; A.lP_at = s.lP_at; A.pmin = s.pmin; A.am = s.am; A.inv2 = s.inv2;
+        A.lxs_pid = s.lxs_pid; A.lu_pid = s.lu_pid;
+        A.la = s.la; A.lxa = s.lxa; A.lva = s.lva;
+        A.lkn = s.lkn; A.err = s.err;
+        const int g = blocks(nF, 128);
+        k_adj_c1<R, RN><<<g, 128, 0, stream>>>(A);
+        KL();
+        k_adj_c2<R, RN><<<g, 128, 0, stream>>>(A);
+        KL();
+        k_adj_b2<R, RN><<<g, 128, 0, stream>>>(A);
+        KL();
+        k_adj_a1<R, RN><<<g, 128, 0, stream>>>(A);
+        KL();
+        k_adj_a2<R, RN><<<g, 128, 0, stream>>>(A);
+        KL();
+        k_adj_fin<<<g, 128, 0, stream>>>(d_fluid_ids, nF, s.lx, s.lx_acc);
+        KL();
+    }
+
+    void adjoint_backward(const double* lam_pos, const double* lam_vel, double* g_pos,
+                          double* g_vel, double* g_nu) override {
+        if (!adj || adj->nsteps == 0)
+            throw ApiError(MPS_ERR_STATE, "no recorded rollout: call mps_adjoint_record first");
+        if (nF == 0) return;
+        AdjState& s = *adj;
+        const size_t T = size_t(nT);
+        const int gT = blocks(nT, 256), gF = blocks(nF, 128);
+        // adjoints of the final state, fluid entries only
+        auto load = [&](const double* src, V4<double>* dst) {
+            CK(cudaMemsetAsync(dst, 0, sizeof(V4<double>) * T, stream));
+            if (!src) return;
+            CK(cudaMemcpyAsync(s.stage, src, 3 * T * sizeof(double), cudaMemcpyDefault, stream));
+            k_adj_in<<<gT, 256, 0, stream>>>(s.stage, nT, s.lxs_pid);
+            KL();
+            k_adj_pick<<<gF, 128, 0, stream>>>(d_fluid_ids, nF, s.lxs_pid, dst);
+            KL();
+        };
+        load(lam_pos, s.lx);
+        load(lam_vel, s.lv);
+        CK(cudaMemsetAsync(s.lx_acc, 0, sizeof(V4<double>) * T, stream));
+        CK(cudaMemsetAsync(s.lkn, 0, sizeof(double), stream));
+        CK(cudaMemsetAsync(s.err, 0, sizeof(int), stream));
+        invalidate_graph();
+        for (int c = s.nck - 1; c >= 0; --c) {
+            restore(s.ck[c]);
+            const int ns = std::min(s.every, s.nsteps - c * s.every);
+            tape_prepare(s.tape[0]);
+            for (int k = 0; k < ns; ++k) tape_body(s.tape[k], k + 1 < ns ? &s.tape[k + 1] : nullptr);
+            for (int k = ns - 1; k >= 0; --k) back_step(s.tape[k]);
+        }
+        auto out = [&](const V4<double>* src, double* dst) {
+            if (!dst) return;
+            k_adj_out<<<gT, 256, 0, stream>>>(src, nT, s.stage);
+            KL();
+            CK(cudaMemcpyAsync(dst, s.stage, 3 * T * sizeof(double), cudaMemcpyDefault, stream));
+        };
+        out(s.lx, g_pos);
+        out(s.lv, g_vel);
+        double lkn = 0;
+        int err = 0;
+        CK(cudaMemcpyAsync(&lkn, s.lkn, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(&err, s.err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        // back to the end of the rollout
+        restore(s.ck[s.nck]);
+        steps = s.steps_end;
+        CK(cudaStreamSynchronize(stream));
+        if (err)
+            throw ApiError(MPS_ERR_OVERFLOW,
+                           std::to_string(err) + " neighbour list(s) of the recorded rollout exceeded "
+                           "their capacity of " + std::to_string(nbK) +
+                           "; the adjoint needs every list within capacity");
+        // kn = knm_vsc / n0 (derive_scene), so d/d knm_vsc = d/d kn / n0
+        if (g_nu) *g_nu = lkn / double(infos[0].n0);
     }
 
     void integrals(int scene, double out[6]) override {

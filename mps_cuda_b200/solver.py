@@ -246,6 +246,34 @@ class MPSBatch:
         check(lib().mps_get_integrals(self._h, scene, out), "mps_get_integrals")
         return np.array(out[:])
 
+    def adjoint_record(self, nsteps: int, checkpoint_every: int = 20):
+        """Advance nsteps steps, keeping the state every checkpoint_every steps."""
+        check(lib().mps_adjoint_record(self._h, int(nsteps), int(checkpoint_every)),
+              "mps_adjoint_record")
+
+    def adjoint_backward(self, lam_pos=None, lam_vel=None, grad_pos=None, grad_vel=None):
+        """Gradients of the recorded rollout's loss given d loss / d (final pos, vel).
+
+        Arrays are (3, n) float64 in particle-id order: numpy arrays, or anything exposing
+        a device pointer through ``data_ptr()`` (torch CUDA tensors). Output arrays are
+        allocated as numpy when not given. Returns (grad_pos0, grad_vel0, grad_nu).
+        """
+        def ptr(a):
+            if a is None:
+                return None
+            if hasattr(a, "data_ptr"):
+                return C.c_void_p(a.data_ptr())
+            assert a.dtype == np.float64 and a.flags.c_contiguous and a.shape == (3, self.n)
+            return a.ctypes.data_as(C.c_void_p)
+        if grad_pos is None:
+            grad_pos = np.empty((3, self.n))
+        if grad_vel is None:
+            grad_vel = np.empty((3, self.n))
+        gnu = C.c_double()
+        check(lib().mps_adjoint_backward(self._h, ptr(lam_pos), ptr(lam_vel), ptr(grad_pos),
+                                         ptr(grad_vel), C.byref(gnu)), "mps_adjoint_backward")
+        return grad_pos, grad_vel, gnu.value
+
 
 class MPS(MPSBatch):
     """One scene, driven with the reference's method names (class.cuh:8-28).

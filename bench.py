@@ -15,7 +15,10 @@ ours      : libmps_b200.so. `value` = device time of K steps (CUDA events on the
             buffers every step; `roofline` = the dominant kernel group's algorithmic bytes
             per launch over its average launch time, timed live with CUDA events;
             `cpu_baseline` = the CPU oracle (OpenMP restatement of the reference's
-            per-particle loops) on a bounded sample of the same workload, rank 0 only.
+            per-particle loops) on a bounded sample of the same workload, rank 0 only;
+            `batched` = 64 uneven scenes in one handle against a per-scene loop;
+            `adjoint` = the rollout adjoint's cost per step against a forward step at the
+            48 000-particle adjoint workload, with its finite-difference agreement.
 reference : the reference's per-particle loops as that OpenMP CPU restatement (the
             reference itself has no CPU implementation), all host threads, rank 0 only;
             `reference_cuda` adds the reference's own CUDA kernels (built for sm_100a from
@@ -372,6 +375,9 @@ def run_ours(args, world, rank, local):
     batched = None
     if not args.no_batched:
         batched = measure_batched(args, stream, flush, min(K, 50))
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = measure_adjoint(stream)
     clk.__exit__(None, None, None)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -393,10 +399,91 @@ def run_ours(args, world, rank, local):
             "e2e": e2e, "gpu_launches": launches,
             "roofline": roofline, "kernel_groups": groups, "cpu_baseline": cpu,
             "batched": batched,
+            "adjoint": adjoint,
             "counters": {k: v for k, v in cnt.items() if k != "kernel_launches"},
         }
         print(json.dumps(line), flush=True)
     g.close()
+
+
+def measure_adjoint(stream):
+    """Adjoint workload: 48 000-particle dam break, FP64, 200 steps, checkpoints every 20.
+
+    forward : device time of one graph-replayed step (CUDA events, 200 steps).
+    adjoint : device time of mps_adjoint_backward over the recorded rollout (segment
+              replays included) per step, CUDA events on the handle's stream.
+    fd      : gradients of the dam-break loss (centroid and mean height beyond x = 0.7 m
+              against the rollout at nu = 2e-6) against central differences: viscosity at
+              the relative step 1e-4, the initial velocities along a seeded random direction
+              at 1e-8 (collision onsets make the rollout piecewise smooth in them).
+    """
+    import math
+
+    import torch
+
+    from mps_cuda_b200 import _lib as L
+    from mps_cuda_b200 import configs
+    from mps_cuda_b200.adjoint import (RolloutProblem, dambreak_loss, loss_target, rollout,
+                                       rollout_loss)
+
+    desc, dt, steps = configs.WORKLOADS["adjoint_l0.01_48k"]
+    pr = RolloutProblem(desc, dt=dt, steps=steps, every=20)
+    f = pr.fluid
+    v0 = pr.vel[:, f].copy()
+    nu = configs.NU
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    h = pr.solver(nu, v0)
+    h.set_stream(stream.cuda_stream)
+    h.set_option(L.OPT_GRAPH, 1)
+    h.step(3)
+    h.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record(stream)
+    h.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd = e0.elapsed_time(e1) / steps
+    h.close()
+
+    h = pr.solver(nu, v0)
+    h.set_stream(stream.cuda_stream)
+    h.set_option(L.OPT_GRAPH, 1)
+    h.adjoint_record(steps, pr.every)
+    lam = np.zeros((3, h.n))
+    lam[:, f] = 1.0
+    h.adjoint_backward(lam, None)  # warm-up
+    e0, e1 = ev(), ev()
+    e0.record(stream)
+    h.adjoint_backward(lam, None)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    bwd = e0.elapsed_time(e1) / steps
+    h.close()
+
+    target = loss_target(pr, 2e-6, v0)
+    nu_t = torch.tensor(nu, dtype=torch.float64, requires_grad=True)
+    vel_t = torch.tensor(v0, dtype=torch.float64, requires_grad=True)
+    pos, _, alive = rollout(nu_t, vel_t, pr)
+    loss = dambreak_loss(pos, alive, torch.tensor(target))
+    loss.backward()
+    gnu, gv = float(nu_t.grad), vel_t.grad.numpy()
+    hn = 1e-4 * nu
+    fd_nu = (rollout_loss(pr, nu + hn, v0, target) - rollout_loss(pr, nu - hn, v0, target)) / (2 * hn)
+    d = np.random.default_rng(14).standard_normal(v0.shape)
+    eps = 1e-8 * float(np.sqrt(np.mean(v0 ** 2)))
+    fd_v = (rollout_loss(pr, nu, v0 + eps * d, target)
+            - rollout_loss(pr, nu, v0 - eps * d, target)) / (2 * eps)
+    ad_v = math.fsum((gv * d).ravel())
+    rel = lambda a, b: abs(a - b) / max(abs(a), abs(b), 1e-300)  # noqa: E731
+    return {"workload": "adjoint_l0.01_48k", "fluid_particles": int(f.size), "steps": steps,
+            "checkpoint_every": pr.every, "precision": "f64",
+            "forward_ms_per_step": fwd, "adjoint_ms_per_step": bwd,
+            "adjoint_over_forward": bwd / fwd,
+            "loss": float(loss.detach()), "grad_nu": gnu, "fd_grad_nu": fd_nu,
+            "fd_rel_err_nu": rel(gnu, fd_nu), "grad_vel0_dir": ad_v, "fd_grad_vel0_dir": fd_v,
+            "fd_rel_err_vel0": rel(ad_v, fd_v),
+            "fd_steps": {"nu": 1e-4, "vel0": 1e-8}}
 
 
 def measure_batched(args, stream, flush, K: int):
@@ -473,6 +560,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     world, rank, local = setup_dist()
     try:

@@ -29,7 +29,8 @@ import pytest
 
 from mps_cuda_b200 import SceneDesc, configs, select_device
 from mps_cuda_b200 import _lib as L
-from mps_cuda_b200.adjoint import RolloutProblem, dambreak_loss, loss_target, rollout
+from mps_cuda_b200.adjoint import (RolloutProblem, dambreak_loss, loss_target, rollout,
+                                   rollout_loss)
 
 pytestmark = pytest.mark.gpu
 
@@ -152,15 +153,7 @@ def test_linear_functional_adjoint_workload():
 
 
 def exact_loss(problem, nu, v0, target):
-    st = problem.run(nu, v0)
-    f = problem.fluid
-    alive = st["typ"][f] == L.FLD
-    p = st["pos"][:, f][:, alive]
-    c = [math.fsum(p[k]) / p.shape[1] for k in range(3)]
-    sel = p[0] > 0.7
-    zbar = math.fsum(p[2][sel]) / int(sel.sum()) if sel.any() else 0.0
-    dc = [c[k] - target[k] for k in range(3)] + [zbar - target[3]]
-    return math.fsum(x * x for x in dc)
+    return rollout_loss(problem, nu, v0, target)
 
 
 def test_dambreak_loss_through_torch_autograd():

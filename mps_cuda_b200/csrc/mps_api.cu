@@ -112,13 +112,13 @@ int mps_derive(const mps_params* p, mps_info* out) {
     if (rc) return rc;
     if (p->precision == 1) {
         mps::SceneDev<double, double> sd;
-        mps::derive_scene<double, double>(*p, 0, 0, 0, sd, *out);
+        mps::derive_scene<double, double>(*p, 0, 0, 0, 0, sd, *out);
     } else if (p->precision == 2) {
         mps::SceneDev<float, double> sd;
-        mps::derive_scene<float, double>(*p, 0, 0, 0, sd, *out);
+        mps::derive_scene<float, double>(*p, 0, 0, 0, 0, sd, *out);
     } else {
         mps::SceneDev<float, float> sd;
-        mps::derive_scene<float, float>(*p, 0, 0, 0, sd, *out);
+        mps::derive_scene<float, float>(*p, 0, 0, 0, 0, sd, *out);
     }
     return MPS_OK;
 }

@@ -71,6 +71,7 @@ __device__ __forceinline__ bool cell_of(const SceneDev<R, RN>& sc, R x, R y, R z
 template <class R> struct RowCtx {
     int ix, iy, iz;
     R dxl, dxh, dyl, dyh, dzl, dzh;
+    float rx, ry, rz;  // position relative to the grid minimum (fine-row geometry)
 };
 
 template <class R, class RN>
@@ -84,7 +85,99 @@ __device__ __forceinline__ RowCtx<R> row_ctx(const SceneDev<R, RN>& sc, R x, R y
     c.dxl = x - xl; c.dxh = (xl + sc.db) - x;
     c.dyl = y - yl; c.dyh = (yl + sc.db) - y;
     c.dzl = z - zl; c.dzh = (zl + sc.db) - z;
+    c.rx = float(x - sc.minc[0]);
+    c.ry = float(y - sc.minc[1]);
+    c.rz = float(z - sc.minc[2]);
     return c;
+}
+
+// Fine cell of a fluid particle: a third of its bucket per axis. t = (x - min) * dbinv is
+// the bucket coordinate of kernel.cu:521-524 and the fine coordinate is fx = int(3 t) + 3;
+// for t >= 0 rounding keeps int(3 t) in [3 int(t), 3 int(t) + 2], so the fine cell lies
+// inside the bucket. The clamp repeats cell_of's for positions outside the grid. Fine cells
+// are numbered bucket-major (27 per bucket, z, y, x inside it), so that consecutive slots
+// stay within one bucket.
+template <class R, class RN>
+__device__ __forceinline__ int fine_cell(const SceneDev<R, RN>& sc, R x, R y, R z, bool& ok) {
+    const R tx = (x - sc.minc[0]) * sc.dbinv, ty = (y - sc.minc[1]) * sc.dbinv,
+            tz = (z - sc.minc[2]) * sc.dbinv;
+    int ix = int(tx) + 1, iy = int(ty) + 1, iz = int(tz) + 1;
+    ok = ix >= 1 && ix <= sc.nbx - 2 && iy >= 1 && iy <= sc.nby - 2 && iz >= 1 && iz <= sc.nbz - 2;
+    ix = min(max(ix, 1), sc.nbx - 2);
+    iy = min(max(iy, 1), sc.nby - 2);
+    iz = min(max(iz, 1), sc.nbz - 2);
+    const int sx = min(max(int(R(3) * tx) + 3, 3 * ix), 3 * ix + 2) - 3 * ix;
+    const int sy = min(max(int(R(3) * ty) + 3, 3 * iy), 3 * iy + 2) - 3 * iy;
+    const int sz = min(max(int(R(3) * tz) + 3, 3 * iz), 3 * iz + 2) - 3 * iz;
+    return sc.fbase + 27 * (iz * sc.nbxy + iy * sc.nbx + ix) + 9 * sz + 3 * sy + sx;
+}
+
+// first / last fine index of the 9 around the bucket (f0 = 3 i - 3) whose cells reach
+// coordinate v; v * ihf + 3 is the fine coordinate
+__device__ __forceinline__ int fine_at(float v, float ihf, int f0) {
+    return int(fminf(fmaxf(fmaf(v, ihf, 3.0f), float(f0)), float(f0 + 8)));
+}
+// distance from v to fine cell f along one axis
+__device__ __forceinline__ float fine_gap(float v, int f, float hf) {
+    const float lo = float(f - 3) * hf;
+    return fmaxf(fmaxf(lo - v, v - (lo + hf)), 0.0f);
+}
+
+// A fluid slot index kept in the w component of a position (the row-ordered copy posf)
+__device__ __forceinline__ float slot_w(int s, float) { return __int_as_float(s); }
+__device__ __forceinline__ double slot_w(int s, double) { return double(s); }
+__device__ __forceinline__ int w_slot(float w) { return __float_as_int(w); }
+__device__ __forceinline__ int w_slot(double w) { return int(w); }
+
+// Row-major number of bucket-major fine cell c (fz * 9 nbxy + fy * 3 nbx + fx): the order
+// of the copy posf, in which one fine row across the 27 buckets is one contiguous range.
+template <class R, class RN>
+__device__ __forceinline__ int fine_rowmajor(const SceneDev<R, RN>& sc, int c) {
+    const int l = c - sc.fbase, b = l / 27, sub = l - 27 * b;
+    const int bz = b / sc.nbxy, by = (b - bz * sc.nbxy) / sc.nbx, bx = b - bz * sc.nbxy - by * sc.nbx;
+    const int fz = 3 * bz + sub / 9, fy = 3 * by + (sub / 3) % 3, fx = 3 * bx + sub % 3;
+    return sc.fbase + fz * (9 * sc.nbxy) + fy * (3 * sc.nbx) + fx;
+}
+
+// Visit the fluid of the 27 buckets around c in fine cells, z, y, x ascending, ascending
+// particle id inside a fine cell, through the row-ordered copy posf (start table csr):
+// f(slot, position) for every particle of the cells within sqrt(B) of the particle. `B` is
+// (radius + margin)^2, the margin (1e-3 of a bucket) covering the float geometry. The
+// neighbours inside the radius, and their order, are those of a walk over every fine cell
+// of the 27 buckets.
+template <class R, class RN, class F>
+__device__ __forceinline__ void for_fluid_ranges(const SceneDev<R, RN>& sc,
+                                                 const int* __restrict__ csr, const RowCtx<R>& c,
+                                                 R B, F&& f) {
+    const float b = float(B), hf = sc.hf, ih = sc.ihf;
+    const float s = sqrtf(b);
+    const int fx0 = 3 * c.ix - 3, fy0 = 3 * c.iy - 3, fz0 = 3 * c.iz - 3;
+    const int nfx = 3 * sc.nbx, nfxy = 9 * sc.nbxy;
+    const int zl = fine_at(c.rz - s, ih, fz0), zh = fine_at(c.rz + s, ih, fz0);
+    for (int fz = zl; fz <= zh; ++fz) {
+        const float gz = fine_gap(c.rz, fz, hf);
+        const float bz = fmaxf(b - gz * gz, 0.0f), sy = sqrtf(bz);
+        const int yl = fine_at(c.ry - sy, ih, fy0), yh = fine_at(c.ry + sy, ih, fy0);
+        for (int fy = yl; fy <= yh; ++fy) {
+            const float gy = fine_gap(c.ry, fy, hf);
+            const float sx = sqrtf(fmaxf(bz - gy * gy, 0.0f));
+            const int xl = fine_at(c.rx - sx, ih, fx0), xh = fine_at(c.rx + sx, ih, fx0);
+            const int row = sc.fbase + fz * nfxy + fy * nfx;
+            f(__ldg(csr + row + xl), __ldg(csr + row + xh + 1));
+        }
+    }
+}
+
+template <class R, class RN, class F>
+__device__ __forceinline__ void for_fluid(const SceneDev<R, RN>& sc, const int* __restrict__ csr,
+                                          const V4<R>* __restrict__ posf, const RowCtx<R>& c, R B,
+                                          F&& f) {
+    for_fluid_ranges(sc, csr, c, B, [&](int lo, int hi) {
+        for (int k = lo; k < hi; ++k) {
+            const V4<R> q = ldg4(posf + k);
+            f(w_slot(q.w), q);
+        }
+    });
 }
 
 // Visit the 27 buckets around c (z, y, x ascending); a row of three x-adjacent buckets is
@@ -179,13 +272,12 @@ __device__ __forceinline__ void visc_sum_mirrors(const SceneDev<R, RN>& sc, cons
 template <class R, class RN>
 __device__ __forceinline__ void visc_sum(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
                                          R x, R y, R z, R ux, R uy, R uz,
-                                         const int* __restrict__ cs,
-                                         const V4<R>* __restrict__ pos,
+                                         const int* __restrict__ csr,
+                                         const V4<R>* __restrict__ posf,
                                          const V4<R>* __restrict__ vel, const MirrorView<R>& m,
                                          R B, R& sx, R& sy, R& sz, int& cf, int& cm) {
-    for_rows(sc, cs, c, B, [&](int j) {
+    for_fluid(sc, csr, posf, c, B, [&](int j, const V4<R>& q) {
         if (j == s) return;
-        V4<R> q = ldg4(pos + j);
         R dx = q.x - x, dy = q.y - y, dz = q.z - z;
         R d2 = dot3(dx, dy, dz, dx, dy, dz);
         if (d2 <= sc.r_le) {  // dist <= r
@@ -205,12 +297,12 @@ __device__ __forceinline__ void visc_sum(const SceneDev<R, RN>& sc, const RowCtx
 template <class R, class RN>
 __device__ __noinline__ void visc_sum_outline(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
                                               R x, R y, R z, R ux, R uy, R uz,
-                                              const int* __restrict__ cs,
-                                              const V4<R>* __restrict__ pos,
+                                              const int* __restrict__ csr,
+                                              const V4<R>* __restrict__ posf,
                                               const V4<R>* __restrict__ vel,
                                               const MirrorView<R>& m, R B, R& sx, R& sy, R& sz,
                                               int& cf, int& cm) {
-    visc_sum(sc, c, s, x, y, z, ux, uy, uz, cs, pos, vel, m, B, sx, sy, sz, cf, cm);
+    visc_sum(sc, c, s, x, y, z, ux, uy, uz, csr, posf, vel, m, B, sx, sy, sz, cf, cm);
 }
 
 // ---- ChkPcl (kernel.cu:481-513); returns false when the particle is deleted --------------
@@ -296,16 +388,15 @@ __device__ __forceinline__ void col_dens_walls_mirrors(const SceneDev<R, RN>& sc
 template <class R, class RN, bool COL, bool DENS>
 __device__ __forceinline__ void col_dens_sum(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
                                              R x, R y, R z, R ux, R uy, R uz,
-                                             const int* __restrict__ cs,
-                                             const V4<R>* __restrict__ pos,
+                                             const int* __restrict__ csr,
+                                             const V4<R>* __restrict__ posf,
                                              const V4<R>* __restrict__ vel,
                                              const WallView<R>& wl, const MirrorView<R>& m,
                                              bool skip, R& wx, R& wy, R& wz, RN& ni, int* cnt) {
     const R inf = R(INFINITY);
     const R Bf = !skip ? inf : (COL && DENS ? sc.skip_rc : (DENS ? sc.skip_rp : sc.skip_rl));
-    for_rows(sc, cs, c, Bf, [&](int j) {
+    for_fluid(sc, csr, posf, c, Bf, [&](int j, const V4<R>& q) {
         if (j == s) return;
-        V4<R> q = ldg4(pos + j);
         R dx = q.x - x, dy = q.y - y, dz = q.z - z;
         R d2 = dot3(dx, dy, dz, dx, dy, dz);
         if (COL && d2 < sc.rlim2) {
@@ -327,13 +418,13 @@ __device__ __forceinline__ void col_dens_sum(const SceneDev<R, RN>& sc, const Ro
 template <class R, class RN, bool COL, bool DENS>
 __device__ __noinline__ void col_dens_sum_outline(const SceneDev<R, RN>& sc, const RowCtx<R>& c,
                                                   int s, R x, R y, R z, R ux, R uy, R uz,
-                                                  const int* __restrict__ cs,
-                                                  const V4<R>* __restrict__ pos,
+                                                  const int* __restrict__ csr,
+                                                  const V4<R>* __restrict__ posf,
                                                   const V4<R>* __restrict__ vel,
                                                   const WallView<R>& wl, const MirrorView<R>& m,
                                                   bool skip, R& wx, R& wy, R& wz, RN& ni,
                                                   int* cnt) {
-    col_dens_sum<R, RN, COL, DENS>(sc, c, s, x, y, z, ux, uy, uz, cs, pos, vel, wl, m, skip, wx,
+    col_dens_sum<R, RN, COL, DENS>(sc, c, s, x, y, z, ux, uy, uz, csr, posf, vel, wl, m, skip, wx,
                                    wy, wz, ni, cnt);
 }
 
@@ -379,15 +470,14 @@ __device__ __forceinline__ void grad_sum_mirrors(const SceneDev<R, RN>& sc, cons
 template <class R, class RN>
 __device__ __forceinline__ void grad_sum(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
                                          int pid_local, R x, R y, R z, R pi,
-                                         const int* __restrict__ cs,
-                                         const V4<R>* __restrict__ pos,
+                                         const int* __restrict__ csr,
+                                         const V4<R>* __restrict__ posf,
                                          const R* __restrict__ prs, const MirrorView<R>& m,
                                          bool skip, R& sx, R& sy, R& sz, int& cf, int& cm) {
     R B = skip ? sc.skip_rp : R(INFINITY);
     R pmin = pi;
-    for_rows(sc, cs, c, B, [&](int j) {
+    for_fluid(sc, csr, posf, c, B, [&](int j, const V4<R>& q) {
         if (j == s) return;
-        V4<R> q = ldg4(pos + j);
         R dx = q.x - x, dy = q.y - y, dz = q.z - z;
         R d2 = dot3(dx, dy, dz, dx, dy, dz);
         if (d2 < sc.rp2) {
@@ -395,9 +485,8 @@ __device__ __forceinline__ void grad_sum(const SceneDev<R, RN>& sc, const RowCtx
             if (pj < pmin) pmin = pj;
         }
     });
-    for_rows(sc, cs, c, B, [&](int j) {
+    for_fluid(sc, csr, posf, c, B, [&](int j, const V4<R>& q) {
         if (j == s) return;
-        V4<R> q = ldg4(pos + j);
         R dx = q.x - x, dy = q.y - y, dz = q.z - z;
         R d2 = dot3(dx, dy, dz, dx, dy, dz);
         if (d2 < sc.rp2) {
@@ -417,11 +506,11 @@ __device__ __forceinline__ void grad_sum(const SceneDev<R, RN>& sc, const RowCtx
 template <class R, class RN>
 __device__ __noinline__ void grad_sum_outline(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
                                               int pid_local, R x, R y, R z, R pi,
-                                              const int* __restrict__ cs,
-                                              const V4<R>* __restrict__ pos,
+                                              const int* __restrict__ csr,
+                                              const V4<R>* __restrict__ posf,
                                               const R* __restrict__ prs, const MirrorView<R>& m,
                                               bool skip, R& sx, R& sy, R& sz, int& cf, int& cm) {
-    grad_sum(sc, c, s, pid_local, x, y, z, pi, cs, pos, prs, m, skip, sx, sy, sz, cf, cm);
+    grad_sum(sc, c, s, pid_local, x, y, z, pi, csr, posf, prs, m, skip, sx, sy, sz, cf, cm);
 }
 
 // ---- MRRinout cull of one mirror (kernel.cu:932-985); true = keep -----------------------

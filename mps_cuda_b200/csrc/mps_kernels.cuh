@@ -37,9 +37,10 @@ template <class R, class RN> struct FluidKeySrc {
         int s = nscene > 1 ? scene_of(sc, nscene, id) : 0;
         V4<R> p = pos[t];
         if (!(isfinite(p.x) && isfinite(p.y) && isfinite(p.z))) atomicAdd(&cnt->err_nan, 1);
-        int ix, iy, iz;
-        if (!cell_of(sc[s], p.x, p.y, p.z, ix, iy, iz)) atomicAdd(&cnt->err_cell, 1);
-        return sc[s].cbase + iz * sc[s].nbxy + iy * sc[s].nbx + ix;
+        bool ok;
+        const int c = fine_cell(sc[s], p.x, p.y, p.z, ok);
+        if (!ok) atomicAdd(&cnt->err_cell, 1);
+        return c;
     }
     __device__ __forceinline__ int id(int t) const { return pid[t]; }
 };
@@ -159,6 +160,64 @@ template <class R> struct MirrorGather {
         dslot[d] = slot[t];
     }
 };
+
+// FluidGather that also writes the row-ordered position copy: an item of fine cell c
+// (bucket-major, starts cs) that lands in slot d goes to posf[csr[rowmajor(c)] + d - cs[c]]
+// with its slot in w. Inside a fine cell both orders are ascending id.
+template <class R, class RN> struct FluidGatherF {
+    FluidGather<R> g;
+    const SceneDev<R, RN>* sc;
+    int nscene;
+    const int* key; const int* cs; const int* csr;
+    V4<R>* posf;
+    __device__ __forceinline__ void operator()(int t, int d) const {
+        g(t, d);
+        if (g.typ[t] != kFLD) return;
+        const int c = key[t];
+        const int id = g.pid[t];
+        const SceneDev<R, RN>& s = sc[nscene > 1 ? scene_of(sc, nscene, id) : 0];
+        const V4<R> p = g.pos[t];
+        posf[__ldg(csr + fine_rowmajor(s, c)) + d - __ldg(cs + c)] = V4<R>{p.x, p.y, p.z, slot_w(d, R(0))};
+    }
+};
+
+// scene holding global fine cell c (scenes are stored in ascending fbase)
+template <class R, class RN>
+__device__ __forceinline__ int scene_of_fine(const SceneDev<R, RN>* sc, int nscene, int c) {
+    int lo = 0, hi = nscene - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&sc[mid].fbase) <= c) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// per-fine-cell counts in row-major order (the last entry counts unlisted items)
+template <class R, class RN>
+__global__ void k_count_rowmajor(const SceneDev<R, RN>* sc, int nscene, const int* __restrict__ count,
+                                 int* __restrict__ count_r, int ncell) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= ncell; c += gridDim.x * blockDim.x) {
+        if (c == ncell) {
+            count_r[c] = count[c];
+        } else {
+            const SceneDev<R, RN>& s = sc[nscene > 1 ? scene_of_fine(sc, nscene, c) : 0];
+            count_r[fine_rowmajor(s, c)] = count[c];
+        }
+    }
+}
+
+// positions of the row-ordered copy from the slots' current positions (the per-method
+// path moves particles in place between bucket builds)
+template <class R>
+__global__ void k_posf_refresh(V4<R>* posf, const V4<R>* __restrict__ pos, const int* __restrict__ csr,
+                               int ncell) {
+    const int n = __ldg(csr + ncell);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const V4<R> q = posf[k];
+        const V4<R> p = pos[w_slot(q.w)];
+        posf[k] = V4<R>{p.x, p.y, p.z, q.w};
+    }
+}
 
 // MirrorGather that also carries the recorded reflection normals
 template <class R> struct MirrorGatherN {
@@ -285,6 +344,9 @@ template <class R, class RN> struct PassArgs {
     // recorded rollouts only: per slot the velocity before ChkPcl's clamp, w = slot state
     // (kTapeOk, kTapeClamped, kTapeDeleted, kTapeDead)
     V4<R>* tape_pre;
+    // fluid positions in row-major fine-cell order, w = slot; csr its fine-cell starts
+    const V4<R>* posf;
+    const int* csr;
 };
 
 // near_wall flag of every bucket of every scene (walls are static: computed once)
@@ -324,28 +386,29 @@ __device__ __forceinline__ int build_list(const PassArgs<R, RN>& a, const SceneD
                                           const RowCtx<R>& c, int s, R x, R y, R z, R thr, R B) {
     int cnt = 0;
     int* __restrict__ nb = a.nb;
-    const V4<R>* __restrict__ pos = a.pos;
+    const V4<R>* __restrict__ posf = a.posf;
     const int nF = a.nF, K = a.nbK;
-    for_rows_ranges(sc, a.cs, c, B, [&](int lo, int hi) {
+    for_fluid_ranges(sc, a.csr, c, B, [&](int lo, int hi) {
         // four independent loads in flight before the first test (latency, not bandwidth,
-        // bounds this loop); candidates are still tested and appended in slot order
-        int j = lo;
-        auto visit = [&](int jj, const V4<R>& q) {
+        // bounds this loop); candidates are still tested and appended in visiting order
+        int k = lo;
+        auto visit = [&](const V4<R>& q) {
             R dx = q.x - x, dy = q.y - y, dz = q.z - z;
-            if (jj != s && dot3(dx, dy, dz, dx, dy, dz) <= thr) {
-                if (cnt < K) nb[size_t(cnt) * nF + s] = jj;
+            const int j = w_slot(q.w);
+            if (j != s && dot3(dx, dy, dz, dx, dy, dz) <= thr) {
+                if (cnt < K) nb[size_t(cnt) * nF + s] = j;
                 ++cnt;
             }
         };
-        for (; j + 4 <= hi; j += 4) {
-            V4<R> q0 = ldg4(pos + j), q1 = ldg4(pos + j + 1), q2 = ldg4(pos + j + 2),
-                  q3 = ldg4(pos + j + 3);
-            visit(j, q0);
-            visit(j + 1, q1);
-            visit(j + 2, q2);
-            visit(j + 3, q3);
+        for (; k + 4 <= hi; k += 4) {
+            V4<R> q0 = ldg4(posf + k), q1 = ldg4(posf + k + 1), q2 = ldg4(posf + k + 2),
+                  q3 = ldg4(posf + k + 3);
+            visit(q0);
+            visit(q1);
+            visit(q2);
+            visit(q3);
         }
-        for (; j < hi; ++j) visit(j, ldg4(pos + j));
+        for (; k < hi; ++k) visit(ldg4(posf + k));
     });
     return cnt;
 }
@@ -422,7 +485,7 @@ __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
         visc_sum_mirrors(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.m, MPS_INF_SKIP(a, sc.skip_r), sx, sy,
                          sz, cm);
     } else {
-        visc_sum_outline(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.cs, a.pos, a.vel, a.m,
+        visc_sum_outline(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.csr, a.posf, a.vel, a.m,
                          MPS_INF_SKIP(a, sc.skip_r), sx, sy, sz, cf, cm);
     }
     R ax = fmaR(sc.kn, sx, sc.g[0]), ay = fmaR(sc.kn, sy, sc.g[1]), az = fmaR(sc.kn, sz, sc.g[2]);
@@ -505,8 +568,8 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
                                                   a.skip != 0, wx, wy, wz, ni, cnt5);
     } else {
         int t5[5] = {0, 0, 0, 0, 0};  // a separate array keeps cnt5 in registers
-        col_dens_sum_outline<R, RN, true, true>(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.cs,
-                                                a.pos, a.vel, a.wl, a.m, a.skip != 0, wx, wy, wz,
+        col_dens_sum_outline<R, RN, true, true>(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.csr,
+                                                a.posf, a.vel, a.wl, a.m, a.skip != 0, wx, wy, wz,
                                                 ni, t5);
 #pragma unroll
         for (int k = 0; k < 5; ++k) cnt5[k] = t5[k];
@@ -606,7 +669,7 @@ __global__ void __launch_bounds__(128) k_pass_c(PassArgs<R, RN> a) {
         grad_sum_mirrors(sc, c, pid - sc.pbase, p.x, p.y, p.z, pmin, a.m, a.skip != 0, sx, sy, sz,
                          cm);
     } else {
-        grad_sum_outline(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, pi, a.cs, a.pos, a.tprs, a.m,
+        grad_sum_outline(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, pi, a.csr, a.posf, a.tprs, a.m,
                          a.skip != 0, sx, sy, sz, cf, cm);
     }
     R ax = (sc.invro * sx) * sc.a3, ay = (sc.invro * sy) * sc.a3, az = (sc.invro * sz) * sc.a3;
@@ -672,7 +735,7 @@ __global__ void __launch_bounds__(128) k_ph_vsc(PassArgs<R, RN> a) {
     RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
     R sx = 0, sy = 0, sz = 0;
     int cf = 0, cm = 0;
-    visc_sum(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.cs, a.pos, a.vel, a.m,
+    visc_sum(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.csr, a.posf, a.vel, a.m,
              MPS_INF_SKIP(a, sc.skip_r), sx, sy, sz, cf, cm);
     a.acc[s] = V4<R>{fmaR(sc.kn, sx, sc.g[0]), fmaR(sc.kn, sy, sc.g[1]), fmaR(sc.kn, sz, sc.g[2]),
                      R(0)};
@@ -717,7 +780,7 @@ __global__ void __launch_bounds__(128) k_ph_col(PassArgs<R, RN> a) {
     R wx = v.x, wy = v.y, wz = v.z;
     RN ni = 0;
     int cnt5[5] = {0, 0, 0, 0, 0};
-    col_dens_sum<R, RN, true, false>(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.cs, a.pos, a.vel,
+    col_dens_sum<R, RN, true, false>(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.csr, a.posf, a.vel,
                                      a.wl, a.m, a.skip != 0, wx, wy, wz, ni, cnt5);
     a.tvel[s] = V4<R>{wx, wy, wz, R(0)};
     if (DIAG) {
@@ -751,7 +814,7 @@ __global__ void __launch_bounds__(128) k_ph_prs(PassArgs<R, RN> a) {
     R wx = 0, wy = 0, wz = 0;
     RN ni = 0;
     int cnt5[5] = {0, 0, 0, 0, 0};
-    col_dens_sum<R, RN, false, true>(sc, c, s, p.x, p.y, p.z, R(0), R(0), R(0), a.cs, a.pos,
+    col_dens_sum<R, RN, false, true>(sc, c, s, p.x, p.y, p.z, R(0), R(0), R(0), a.csr, a.posf,
                                      a.vel, a.wl, a.m, a.skip != 0, wx, wy, wz, ni, cnt5);
     a.prs[s] = eos(sc, ni);
     if (DIAG) {
@@ -774,7 +837,7 @@ __global__ void __launch_bounds__(128) k_ph_grd(PassArgs<R, RN> a) {
     RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
     R sx = 0, sy = 0, sz = 0;
     int cf = 0, cm = 0;
-    grad_sum(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, a.prs[s], a.cs, a.pos, a.prs, a.m,
+    grad_sum(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, a.prs[s], a.csr, a.posf, a.prs, a.m,
              a.skip != 0, sx, sy, sz, cf, cm);
     a.acc[s] = V4<R>{(sc.invro * sx) * sc.a3, (sc.invro * sy) * sc.a3, (sc.invro * sz) * sc.a3,
                      R(0)};
@@ -959,7 +1022,7 @@ __global__ void k_store_walls(IdState<R> st, const SceneDev<R, RN>* scs, int nsc
     st.typ[id] = wtyp[w];
 }
 
-// per-scene integrals over the listed fluid slots [cs[cbase], cs[cbase + nbxyz])
+// per-scene integrals over the listed fluid slots [cs[fbase], cs[fbase + 27 nbxyz])
 __device__ __forceinline__ void atomic_max_double(double* a, double v) {
     unsigned long long* p = reinterpret_cast<unsigned long long*>(a);
     unsigned long long old = *p;
@@ -975,7 +1038,7 @@ __global__ void k_integrals(const SceneDev<R, RN>* scs, const int* cs, const V4<
                             const V4<R>* vel, const int8_t* typ, const int* nbxyz, double* out) {
     const int sidx = blockIdx.y;
     const SceneDev<R, RN>& sc = scs[sidx];
-    const int lo = cs[sc.cbase], hi = cs[sc.cbase + nbxyz[sidx]];
+    const int lo = cs[sc.fbase], hi = cs[sc.fbase + 27 * nbxyz[sidx]];
     double cx = 0, cy = 0, cz = 0, ke = 0, fr = -1e300, n = 0;
     for (int s = lo + blockIdx.x * blockDim.x + threadIdx.x; s < hi; s += gridDim.x * blockDim.x) {
         if (typ[s] != kFLD) continue;

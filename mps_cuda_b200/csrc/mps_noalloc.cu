@@ -94,7 +94,7 @@ int run(const mps_params& p, int n, const int8_t* typ, const void* pos, int32_t*
         int32_t* order, int32_t* start, cudaStream_t st) {
     SceneDev<R, R> sc;
     mps_info inf;
-    derive_scene<R, R>(p, 0, 0, n, sc, inf);
+    derive_scene<R, R>(p, 0, 0, 0, n, sc, inf);
     const int C = inf.nbxyz;
     if (C > MPS_NOALLOC_MAX_BUCKETS) return MPS_ERR_OVERFLOW;
     int dev = 0, *base = nullptr;

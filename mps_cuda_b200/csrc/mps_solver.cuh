@@ -66,8 +66,8 @@ template <class R> static R sqrt_threshold(R r, bool le) {
 }
 
 template <class R, class RN>
-static void derive_scene(const mps_params& p, int cbase, int pbase, int pcount, SceneDev<R, RN>& s,
-                         mps_info& inf) {
+static void derive_scene(const mps_params& p, int cbase, int fbase, int pbase, int pcount,
+                         SceneDev<R, RN>& s, mps_info& inf) {
     std::memset(&s, 0, sizeof(s));
     const R l0 = R(p.pcl_dst);
     R maxc[3];
@@ -87,6 +87,9 @@ static void derive_scene(const mps_params& p, int cbase, int pbase, int pcount, 
     s.cbase = cbase;
     s.pbase = pbase;
     s.pcount = pcount;
+    s.fbase = fbase;
+    s.ihf = float(3.0 * double(dbinv));  // fine cell f spans t in [(f - 3) / 3, (f - 2) / 3)
+    s.hf = float(1.0 / (3.0 * double(dbinv)));
     // lattice sums, kernel.cu:336-366
     R tn0 = 0, tn0g = 0, tl = 0, tlg = 0;
     int cnt = 0;
@@ -201,7 +204,7 @@ struct SolverBase {
     virtual ~SolverBase() {}
     int dev = 0;
     cudaStream_t stream = 0, own_stream = 0;
-    int nscene = 0, nT = 0, nF = 0, nW = 0, C = 0, cap = 0;
+    int nscene = 0, nT = 0, nF = 0, nW = 0, C = 0, CF = 0, cap = 0;
     int precision = 0;
     std::vector<mps_info> infos;
     std::vector<int> counts;
@@ -248,6 +251,10 @@ template <class R, class RN> class Solver final : public SolverBase {
     MirrorBuf<R> U, M1, M2;
     int *mcs1, *mcs2;
     int* cs;
+    // fluid positions in row-major fine-cell order (slot in w) and that order's cell starts
+    V4<R>* posf;
+    int *csr, *count_r;
+    bool posf_stale = false;  // particles moved in place since the copy was made
     // bucket-build scratch
     int *key, *rnk, *seg, *count, *part;
     int* d_fluid_ids;
@@ -338,6 +345,9 @@ template <class R, class RN> class Solver final : public SolverBase {
 
     int dead() const { return C; }
     int L() const { return C + 1; }
+    // fluid: fine cells
+    int deadF() const { return CF; }
+    int LF() const { return CF + 1; }
     int blocks(int n, int b) const { return std::max(1, (n + b - 1) / b); }
 
     void init(int ns, const mps_params* p, const int32_t* cnts, const int8_t* typ_in,
@@ -354,12 +364,18 @@ template <class R, class RN> class Solver final : public SolverBase {
         hsc.resize(ns);
         infos.resize(ns);
         int cb = 0, pb = 0;
+        long long fb = 0;
         for (int s = 0; s < ns; ++s) {
-            derive_scene<R, RN>(p[s], cb, pb, cnts[s], hsc[s], infos[s]);
+            derive_scene<R, RN>(p[s], cb, int(fb), pb, cnts[s], hsc[s], infos[s]);
             cb += infos[s].nbxyz;
+            fb += 27LL * infos[s].nbxyz;
             pb += cnts[s];
         }
+        if (fb >= (1LL << 31) - 2)
+            throw ApiError(MPS_ERR_OVERFLOW, "the fine cell grid needs " + std::to_string(fb) +
+                                                 " cells, more than an int32 index holds");
         C = cb;
+        CF = int(fb);
         // classify particles: walls inside the padded box are static walls, everything
         // else is a fluid-class particle; RdDat drops what lies outside (kernel.cu:117)
         std::vector<int8_t> ty(typ_in, typ_in + nT);
@@ -422,7 +438,7 @@ template <class R, class RN> class Solver final : public SolverBase {
             KL();
             WallKeySrc<R, RN> ks{d_sc, nscene, dead(), tw_pos, tw_id};
             WallGather<R> g{tw_pos, tw_nrm, tw_vel, tw_id, tw_typ, w_pos, w_nrm, w_vel, w_id, w_typ};
-            bin(ks, g, nullptr, nW, wcs);
+            bin(ks, g, nullptr, nW, wcs, L());
             WallView<R> wl = wall_view();
             k_surface_edge<R, RN><<<blocks(nW, 128), 128, 0, stream>>>(d_sc, nscene, nW, wl, w_id,
                                                                        w_se);
@@ -464,7 +480,10 @@ template <class R, class RN> class Solver final : public SolverBase {
         w_typ = ar.template get<int8_t>(W);
         w_se = ar.template get<int8_t>(W);
         wcs = ar.template get<int>(L() + 1);
-        cs = ar.template get<int>(L() + 1);
+        cs = ar.template get<int>(size_t(LF()) + 1);
+        csr = ar.template get<int>(size_t(LF()) + 1);
+        count_r = ar.template get<int>(size_t(LF()));
+        posf = ar.template get<V4<R>>(F);
         for (MirrorBuf<R>* b : {&U, &M1, &M2}) {
             b->pos = ar.template get<V4<R>>(cap);
             b->slot = ar.template get<int>(cap);
@@ -475,8 +494,8 @@ template <class R, class RN> class Solver final : public SolverBase {
         key = ar.template get<int>(items);
         rnk = ar.template get<int>(items);
         seg = ar.template get<int>(items);
-        count = ar.template get<int>(L());
-        part = ar.template get<int>((L() + kScanTile - 1) / kScanTile + 1);
+        count = ar.template get<int>(size_t(LF()));  // fine cells outnumber buckets 27:1
+        part = ar.template get<int>((size_t(LF()) + kScanTile - 1) / kScanTile + 1);
         d_fluid_ids = ar.template get<int>(F);
         d_wall_ids = ar.template get<int>(W);
         d_nF = ar.template get<int>(1);
@@ -503,37 +522,68 @@ template <class R, class RN> class Solver final : public SolverBase {
     }
 
     // ---- bucket build ------------------------------------------------------------------
-    template <class Src, class G> void bin(Src src, G g, const int* n_ptr, int n_max, int* out_cs) {
-        CK(cudaMemsetAsync(count, 0, sizeof(int) * L(), stream));
+    // bucket build over `ncell` cells (the last one, `ncell - 1`, holds unlisted items)
+    template <class Src, class G>
+    void bin(Src src, G g, const int* n_ptr, int n_max, int* out_cs, int ncell) {
+        CK(cudaMemsetAsync(count, 0, sizeof(int) * size_t(ncell), stream));
         if (n_max > 0) {
             int grid = std::min(blocks(n_max, 256), 148 * 32);
             k_bin_key<Src><<<grid, 256, 0, stream>>>(src, n_ptr, n_max, key, rnk, count, cnt);
             KL();
         }
-        int nb = (L() + kScanTile - 1) / kScanTile;
-        k_scan_reduce<<<nb, kScanThreads, 0, stream>>>(count, L(), part);
+        int nb = (ncell + kScanTile - 1) / kScanTile;
+        k_scan_reduce<<<nb, kScanThreads, 0, stream>>>(count, ncell, part);
         KL();
-        k_scan_apply<<<nb, kScanThreads, 0, stream>>>(count, L(), part, out_cs);
+        k_scan_apply<<<nb, kScanThreads, 0, stream>>>(count, ncell, part, out_cs);
         KL();
         if (n_max > 0) {
             int grid = std::min(blocks(n_max, 256), 148 * 32);
             k_bin_seg<Src><<<grid, 256, 0, stream>>>(src, n_ptr, n_max, key, rnk, out_cs, seg);
             KL();
             k_bin_fin<Src, G><<<grid, 256, 0, stream>>>(src, g, n_ptr, n_max, key, rnk, out_cs, seg,
-                                                        dead());
+                                                        ncell - 1);
             KL();
         }
     }
 
     // fluid bucket build from (pos, vel, typ) sources into S2, then S <-> S2
+    // The sorted state S2 is bucket-major in fine cells (start table cs); the same build
+    // also writes the row-major copy posf (start table csr) that the neighbour walks read.
     void bin_fluid(const V4<R>* pos, const V4<R>* vel, const V4<R>* acc, const R* prs,
                    const R* pav, const int* pid, const int8_t* typ) {
         Scope sc_(this, MPS_K_BIN_FLUID);
-        FluidKeySrc<R, RN> ks{d_sc, nscene, dead(), pos, typ, pid};
-        FluidGather<R> g{pos, vel, acc, prs, pav, pid, typ,
-                         S2.pos, S2.vel, S2.acc, S2.prs, S2.pav, S2.pid, S2.typ};
-        bin(ks, g, nullptr, nF, cs);
+        FluidKeySrc<R, RN> ks{d_sc, nscene, deadF(), pos, typ, pid};
+        FluidGatherF<R, RN> g{{pos, vel, acc, prs, pav, pid, typ, S2.pos, S2.vel, S2.acc, S2.prs,
+                               S2.pav, S2.pid, S2.typ},
+                              d_sc, nscene, key, cs, csr, posf};
+        const int ncell = LF();
+        CK(cudaMemsetAsync(count, 0, sizeof(int) * size_t(ncell), stream));
+        const int grid = std::min(blocks(std::max(nF, 1), 256), 148 * 32);
+        if (nF > 0) {
+            k_bin_key<FluidKeySrc<R, RN>><<<grid, 256, 0, stream>>>(ks, nullptr, nF, key, rnk, count, cnt);
+            KL();
+        }
+        k_count_rowmajor<R, RN><<<std::min(blocks(ncell, 256), 148 * 16), 256, 0, stream>>>(
+            d_sc, nscene, count, count_r, ncell - 1);
+        KL();
+        const int nb = (ncell + kScanTile - 1) / kScanTile;
+        k_scan_reduce<<<nb, kScanThreads, 0, stream>>>(count, ncell, part);
+        KL();
+        k_scan_apply<<<nb, kScanThreads, 0, stream>>>(count, ncell, part, cs);
+        KL();
+        k_scan_reduce<<<nb, kScanThreads, 0, stream>>>(count_r, ncell, part);
+        KL();
+        k_scan_apply<<<nb, kScanThreads, 0, stream>>>(count_r, ncell, part, csr);
+        KL();
+        if (nF > 0) {
+            k_bin_seg<FluidKeySrc<R, RN>><<<grid, 256, 0, stream>>>(ks, nullptr, nF, key, rnk, cs, seg);
+            KL();
+            k_bin_fin<FluidKeySrc<R, RN>, FluidGatherF<R, RN>><<<grid, 256, 0, stream>>>(
+                ks, g, nullptr, nF, key, rnk, cs, seg, deadF());
+            KL();
+        }
         std::swap(S, S2);
+        posf_stale = false;
     }
 
     void mkbkt(bool with_acc) {
@@ -545,16 +595,18 @@ template <class R, class RN> class Solver final : public SolverBase {
         Scope sc_(this, MPS_K_BIN_MIRROR);
         MirrorKeySrc<R, RN> ks{d_sc, nscene, dead(), U.pos, U.slot};
         MirrorGather<R> g{U.pos, U.slot, dst.pos, dst.slot};
-        bin(ks, g, &cnt->mirror_raw, cap, dcs);
+        bin(ks, g, &cnt->mirror_raw, cap, dcs, L());
     }
 
     WallView<R> wall_view() const { return WallView<R>{wcs, w_pos, w_nrm, w_vel, w_se, w_typ}; }
 
     PassArgs<R, RN> args(const MirrorBuf<R>& m, const int* mcs) {
         PassArgs<R, RN> a;
-        a.sc = d_sc; a.nscene = nscene; a.nF = nF; a.dead = dead();
+        a.sc = d_sc; a.nscene = nscene; a.nF = nF; a.dead = deadF();
         a.skip = (skip_opt && sorted) ? 1 : 0;
         a.cs = cs;
+        a.posf = posf;
+        a.csr = csr;
         a.pos = S.pos; a.vel = S.vel; a.acc = S.acc; a.prs = S.prs; a.pav = S.pav; a.pid = S.pid;
         a.typ = S.typ;
         a.tpos = t_pos; a.tvel = t_vel; a.tprs = t_prs; a.ttyp = t_typ;
@@ -727,6 +779,12 @@ template <class R, class RN> class Solver final : public SolverBase {
         auto need_lists = [&]() {
             if (!lists_valid)
                 throw ApiError(MPS_ERR_STATE, "bucket lists are not built: run MPS_PHASE_MKBKT first");
+            if (posf_stale) {  // the lists stay, the positions read through them are current
+                k_posf_refresh<R><<<std::min(blocks(std::max(nF, 1), 256), 148 * 8), 256, 0, stream>>>(
+                    posf, S.pos, csr, deadF());
+                KL();
+                posf_stale = false;
+            }
         };
         m1_valid = false;
         switch (ph) {
@@ -763,6 +821,7 @@ template <class R, class RN> class Solver final : public SolverBase {
                 k_ph_uppcl1<R, RN><<<gb, block, 0, stream>>>(a);
                 KL();
                 sorted = false;
+                posf_stale = true;
                 acc_dirty = true;
                 break;
             case MPS_PHASE_CHKCOL:
@@ -791,6 +850,7 @@ template <class R, class RN> class Solver final : public SolverBase {
                 k_ph_uppcl2<R, RN><<<gb, block, 0, stream>>>(a);
                 KL();
                 sorted = false;
+                posf_stale = true;
                 acc_dirty = true;
                 break;
             default:
@@ -1045,7 +1105,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     void bin_mirrors_n(V4<R>* dpos, int* dslot, V4<R>* dnrm, int* dcs) {
         MirrorKeySrc<R, RN> ks{d_sc, nscene, dead(), U.pos, U.slot};
         MirrorGatherN<R> g{U.pos, U.slot, adj->unrm, dpos, dslot, dnrm};
-        bin(ks, g, &cnt->mirror_raw, cap, dcs);
+        bin(ks, g, &cnt->mirror_raw, cap, dcs, L());
     }
 
     PassArgs<R, RN> tape_args(const V4<R>* mpos, const int* mslot, const int* mcs, int* nbl,

@@ -1,11 +1,12 @@
 // mps_types.h -- host/device data layout of the B200 MPS solver.
 //
 // Particle state lives in HBM as arrays of 4-wide vectors (16 B per float particle,
-// 32 B per double particle) sorted by bucket: bucket-major in the reference's bucket
-// order ib = iz*nBxy + iy*nBx + ix (kernel.cu:521-524), ascending particle id inside a
-// bucket. Walls are static and kept in their own sorted arrays; mirrors are a compact
-// list sorted by (bucket, slot id) instead of the reference's NumMRR slots per particle
-// (kernel.cu:96-103).
+// 32 B per double particle). Fluid is sorted by the reference's bucket, then by fine cell
+// inside it (a third of a bucket per axis), ascending particle id inside a fine cell, so
+// that a neighbour walk reads only the fine cells its radius reaches. Walls are static and sorted
+// by the reference's bucket order ib = iz*nBxy + iy*nBx + ix (kernel.cu:521-524), ascending
+// id inside a bucket; mirrors are a compact list sorted by (bucket, slot id) instead of
+// the reference's NumMRR slots per particle (kernel.cu:96-103).
 #pragma once
 #include <stdint.h>
 
@@ -33,7 +34,11 @@ template <class R, class RN> struct SceneDev {
     int cbase;        // first global bucket of this scene
     int pbase;        // first global particle id of this scene
     int pcount;       // particles of this scene
-    int pad0;
+    // fluid lists use fine cells, a third of a bucket per axis and nested in the buckets,
+    // numbered fbase + 27 * bucket + 9 sz + 3 sy + sx (sub-cell s = int(3 t) + 3 - 3 i,
+    // t as for the bucket index i)
+    int fbase, pad1, pad2;
+    float hf, ihf;    // fine cell width (bucket width / 3) and its inverse
     R r, r2, r_le;    // Laplacian radius; r_le = largest t with sqrt(t) <= r
     R rp, rp2, rp_lt; // gradient radius; rp_lt = largest t with sqrt(t) < rp
     R rlim2, rlimw2;  // collision radii (kernel.cu:370-371, 1184-1185)

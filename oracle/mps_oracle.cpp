@@ -23,6 +23,11 @@
 // run-to-run varying neighbour order, kernel.cu:525-527):
 //   * bucket lists are ordered by ascending particle id (mirror slot id for mirrors);
 //     the 27 buckets are walked z, y, x ascending as in every reference loop;
+//   * fluid neighbours are visited in fine cells, a third of a bucket per axis and nested
+//     in the buckets (fine x = int(3 t) + 3 with t the bucket coordinate): the 9 x 9 x 9
+//     fine cells of the 27 buckets z, y, x ascending, ascending id inside a fine cell.
+//     The candidates are the reference's (the particles of the 27 buckets); only the
+//     order of the sums is fixed this way;
 //   * ChkCol visits fluid neighbours, then wall neighbours, then mirrors;
 //   * arithmetic is written with explicit fma where a product feeds a sum (the forms an
 //     FMA-contracting compiler produces) and is built with -ffp-contract=off, so every
@@ -70,6 +75,7 @@ struct Oracle {
     R l0, r, r2, rp, rp2, db, dbinv;
     R minc[3], maxc[3], lo[3], hi[3], g[3];
     int nbx, nby, nbz, nbxy, nbxyz;
+    int nfx, nfy, nfz, nfxy, nfxyz;  // fine cells: a third of a bucket per axis
     R n0, lmd, n0_grad, lmd_grad;
     int numn0_grad;
     RN n0_grad_n, prs_coef_n, pmax_n, rho_n;
@@ -83,6 +89,8 @@ struct Oracle {
     std::vector<R> mx, my, mz, mvx, mvy, mvz, mprs;
     // bucket lists: particles (fluid + walls, not GST) and mirrors, ascending id per bucket
     std::vector<int> cstart, clist, mstart, mlist, cell_of;
+    // fluid lists over fine cells, ascending id per fine cell
+    std::vector<int> fstart, flist;
     // diagnostics
     std::vector<int32_t> diag;
     std::vector<R> ndens;
@@ -108,6 +116,11 @@ struct Oracle {
         nbz = int((maxc[2] - minc[2]) * dbinv) + 3;
         nbxy = nbx * nby;
         nbxyz = nbxy * nbz;
+        nfx = 3 * nbx;
+        nfy = 3 * nby;
+        nfz = 3 * nbz;
+        nfxy = nfx * nfy;
+        nfxyz = nfxy * nfz;
         // SetPara lattice sums, kernel.cu:336-366
         R tn0 = 0, tn0g = 0, tl = 0, tlg = 0;
         int cnt = 0;
@@ -180,6 +193,14 @@ struct Oracle {
         iz = int((z - minc[2]) * dbinv) + 1;
         return iz * nbxy + iy * nbx + ix;
     }
+    // fine cell inside bucket (ix, iy, iz): fx = int(3 t) + 3, t = (x - minc) * dbinv
+    inline int fine3(R x, R y, R z, int ix, int iy, int iz) const {
+        const R tx = (x - minc[0]) * dbinv, ty = (y - minc[1]) * dbinv, tz = (z - minc[2]) * dbinv;
+        const int fx = std::min(std::max(int(R(3) * tx) + 3, 3 * ix), 3 * ix + 2);
+        const int fy = std::min(std::max(int(R(3) * ty) + 3, 3 * iy), 3 * iy + 2);
+        const int fz = std::min(std::max(int(R(3) * tz) + 3, 3 * iz), 3 * iz + 2);
+        return fz * nfxy + fy * nfx + fx;
+    }
     inline bool cell_ok(int ix, int iy, int iz) const {
         return ix >= 1 && ix <= nbx - 2 && iy >= 1 && iy <= nby - 2 && iz >= 1 && iz <= nbz - 2;
     }
@@ -233,6 +254,21 @@ struct Oracle {
         std::vector<int> fill(cstart.begin(), cstart.end() - 1);
         for (int i = 0; i < n; ++i)
             if (cell_of[i] >= 0) clist[fill[cell_of[i]]++] = i;
+        // fluid by fine cell
+        fstart.assign(size_t(nfxyz) + 1, 0);
+        std::vector<int> fc(n, -1);
+        for (int i = 0; i < n; ++i) {
+            if (typ[i] != FLD || cell_of[i] < 0) continue;
+            int ix, iy, iz;
+            cell3(px[i], py[i], pz[i], ix, iy, iz);
+            fc[i] = fine3(px[i], py[i], pz[i], ix, iy, iz);
+            fstart[fc[i] + 1]++;
+        }
+        for (int c = 0; c < nfxyz; ++c) fstart[c + 1] += fstart[c];
+        flist.assign(fstart[nfxyz], 0);
+        std::vector<int> ffill(fstart.begin(), fstart.end() - 1);
+        for (int i = 0; i < n; ++i)
+            if (fc[i] >= 0) flist[ffill[fc[i]]++] = i;
     }
 
     // mirror list over MRR slots in ascending slot order (d_MkBkt_MRR, kernel.cu:916-929)
@@ -265,6 +301,36 @@ struct Oracle {
                     int jb = jz * nbxy + jy * nbx + jx;
                     for (int k = st[jb]; k < st[jb + 1]; ++k) f(li[k]);
                 }
+    }
+
+    // visit the fluid of the 27 buckets around (ix, iy, iz) in fine cells, z, y, x
+    // ascending; fine cells farther than radius (+ 1e-3 of a bucket) from (x, y, z) hold no
+    // neighbour and are passed over
+    template <class F> inline void for_fluid(R x, R y, R z, int ix, int iy, int iz, R radius,
+                                             F&& f) const {
+        const double h = 1.0 / (3.0 * double(dbinv)), m = double(radius) + 1e-3 * double(db);
+        const double rx = double(x) - double(minc[0]), ry = double(y) - double(minc[1]),
+                     rz = double(z) - double(minc[2]);
+        auto gap = [&](double v, int fc) {
+            const double a = (fc - 3) * h;
+            return std::max({a - v, v - (a + h), 0.0});
+        };
+        for (int fz = 3 * iz - 3; fz <= 3 * iz + 5; ++fz) {
+            if (fz < 0 || fz >= nfz) continue;
+            const double gz = gap(rz, fz);
+            for (int fy = 3 * iy - 3; fy <= 3 * iy + 5; ++fy) {
+                if (fy < 0 || fy >= nfy) continue;
+                const double gy = gap(ry, fy);
+                if (gy * gy + gz * gz > m * m) continue;
+                for (int fx = 3 * ix - 3; fx <= 3 * ix + 5; ++fx) {
+                    if (fx < 0 || fx >= nfx) continue;
+                    const double gx = gap(rx, fx);
+                    if (gx * gx + gy * gy + gz * gz > m * m) continue;
+                    const int c = fz * nfxy + fy * nfx + fx;
+                    for (int k = fstart[c]; k < fstart[c + 1]; ++k) f(flist[k]);
+                }
+            }
+        }
     }
 
     // ---- Surface_Edge (kernel.cu:553-668) ----------------------------------------------
@@ -422,7 +488,7 @@ struct Oracle {
             int cf = 0, cm = 0;
             int ix, iy, iz;
             cell3(x, y, z, ix, iy, iz);
-            for_nb(cstart, clist, ix, iy, iz, [&](int j) {
+            for_fluid(x, y, z, ix, iy, iz, r, [&](int j) {
                 if (j == i || typ[j] != FLD) return;
                 R qx = px[j] - x, qy = py[j] - y, qz = pz[j] - z;
                 R d2 = dot3(qx, qy, qz, qx, qy, qz);
@@ -506,7 +572,7 @@ struct Oracle {
                     wx = fmar(-qx, f, wx); wy = fmar(-qy, f, wy); wz = fmar(-qz, f, wz);
                 }
             };
-            for_nb(cstart, clist, ix, iy, iz, [&](int j) {
+            for_fluid(x, y, z, ix, iy, iz, std::sqrt(rlim2), [&](int j) {
                 if (j == i || typ[j] != FLD) return;
                 R qx = px[j] - x, qy = py[j] - y, qz = pz[j] - z;
                 R d2 = dot3(qx, qy, qz, qx, qy, qz);
@@ -554,7 +620,7 @@ struct Oracle {
                 }
                 return false;
             };
-            for_nb(cstart, clist, ix, iy, iz, [&](int j) {
+            for_fluid(x, y, z, ix, iy, iz, rp, [&](int j) {
                 if (j == i || typ[j] != FLD) return;
                 R qx = px[j] - x, qy = py[j] - y, qz = pz[j] - z;
                 if (add(dot3(qx, qy, qz, qx, qy, qz))) ++cf;
@@ -586,7 +652,7 @@ struct Oracle {
             R pmin = prs[i];
             int ix, iy, iz;
             cell3(x, y, z, ix, iy, iz);
-            for_nb(cstart, clist, ix, iy, iz, [&](int j) {
+            for_fluid(x, y, z, ix, iy, iz, rp, [&](int j) {
                 if (j == i || typ[j] != FLD) return;
                 R qx = px[j] - x, qy = py[j] - y, qz = pz[j] - z;
                 R d2 = dot3(qx, qy, qz, qx, qy, qz);
@@ -596,7 +662,7 @@ struct Oracle {
             });
             R sx = 0, sy = 0, sz = 0;
             int cf = 0, cm = 0;
-            for_nb(cstart, clist, ix, iy, iz, [&](int j) {
+            for_fluid(x, y, z, ix, iy, iz, rp, [&](int j) {
                 if (j == i || typ[j] != FLD) return;
                 R qx = px[j] - x, qy = py[j] - y, qz = pz[j] - z;
                 R d2 = dot3(qx, qy, qz, qx, qy, qz);

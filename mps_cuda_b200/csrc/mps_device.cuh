@@ -293,18 +293,6 @@ __device__ __forceinline__ void visc_sum(const SceneDev<R, RN>& sc, const RowCtx
     visc_sum_mirrors(sc, c, x, y, z, ux, uy, uz, m, B, sx, sy, sz, cm);
 }
 
-// out-of-line copy for the rare slot whose neighbour list overflowed its capacity
-template <class R, class RN>
-__device__ __noinline__ void visc_sum_outline(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
-                                              R x, R y, R z, R ux, R uy, R uz,
-                                              const int* __restrict__ csr,
-                                              const V4<R>* __restrict__ posf,
-                                              const V4<R>* __restrict__ vel,
-                                              const MirrorView<R>& m, R B, R& sx, R& sy, R& sz,
-                                              int& cf, int& cm) {
-    visc_sum(sc, c, s, x, y, z, ux, uy, uz, csr, posf, vel, m, B, sx, sy, sz, cf, cm);
-}
-
 // ---- ChkPcl (kernel.cu:481-513); returns false when the particle is deleted --------------
 template <class R, class RN>
 __device__ __forceinline__ bool chkpcl(const SceneDev<R, RN>& sc, R x, R y, R z, R& ux, R& uy,

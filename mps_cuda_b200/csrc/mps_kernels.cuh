@@ -453,41 +453,57 @@ __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
     RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
     R sx = 0, sy = 0, sz = 0;
     int cf = 0, cm = 0;
-    const int n = build_list(a, sc, c, s, p.x, p.y, p.z, sc.r_le, MPS_INF_SKIP(a, sc.skip_r));
-    if (TAPE) a.nbcnt[s] = n;
-    if (n <= a.nbK) {
-        const int* __restrict__ nb = a.nb + s;
-        const V4<R>* __restrict__ pos = a.pos;
+    {
+        // one walk over the candidates: test, then the velocity term of each neighbour in
+        // visiting order; four candidates' positions and the accepted ones' velocities in
+        // flight at a time
+        const V4<R>* __restrict__ posf = a.posf;
         const V4<R>* __restrict__ vel = a.vel;
-        const size_t st = a.nF;
-        const R two_l0 = sc.two_l0;
-        auto add = [&](const V4<R>& q, const V4<R>& u) {
+        const R two_l0 = sc.two_l0, r_le = sc.r_le;
+        int* __restrict__ nb = a.nb;
+        const int nF = a.nF, K = a.nbK;
+        auto near = [&](const V4<R>& q, int j, R& d2) {
             R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-            R d2 = dot3(dx, dy, dz, dx, dy, dz);
+            d2 = dot3(dx, dy, dz, dx, dy, dz);
+            return j != s && d2 <= r_le;  // dist <= r
+        };
+        auto add = [&](R d2, const V4<R>& u, int j) {
             R d = sqrtR(d2);
             R w = two_l0 / (d2 * d);
             sx = fmaR(u.x - v.x, w, sx);
             sy = fmaR(u.y - v.y, w, sy);
             sz = fmaR(u.z - v.z, w, sz);
+            if (TAPE && cf < K) nb[size_t(cf) * nF + s] = j;
+            ++cf;
         };
-        int k = 0;
-        for (; k + 2 <= n; k += 2) {  // two neighbours' loads in flight, summed in order
-            const int j0 = nb[k * st], j1 = nb[(k + 1) * st];
-            V4<R> q0 = ldg4(pos + j0), u0 = ldg4(vel + j0), q1 = ldg4(pos + j1), u1 = ldg4(vel + j1);
-            add(q0, u0);
-            add(q1, u1);
-        }
-        if (k < n) {
-            const int j = nb[k * st];
-            add(ldg4(pos + j), ldg4(vel + j));
-        }
-        cf = n;
-        visc_sum_mirrors(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.m, MPS_INF_SKIP(a, sc.skip_r), sx, sy,
-                         sz, cm);
-    } else {
-        visc_sum_outline(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.csr, a.posf, a.vel, a.m,
-                         MPS_INF_SKIP(a, sc.skip_r), sx, sy, sz, cf, cm);
+        const V4<R> z4{R(0), R(0), R(0), R(0)};
+        for_fluid_ranges(sc, a.csr, c, MPS_INF_SKIP(a, sc.skip_r), [&](int lo, int hi) {
+            int k = lo;
+            for (; k + 4 <= hi; k += 4) {
+                const V4<R> q0 = ldg4(posf + k), q1 = ldg4(posf + k + 1), q2 = ldg4(posf + k + 2),
+                            q3 = ldg4(posf + k + 3);
+                const int j0 = w_slot(q0.w), j1 = w_slot(q1.w), j2 = w_slot(q2.w), j3 = w_slot(q3.w);
+                R e0, e1, e2, e3;
+                const bool t0 = near(q0, j0, e0), t1 = near(q1, j1, e1), t2 = near(q2, j2, e2),
+                           t3 = near(q3, j3, e3);
+                const V4<R> u0 = t0 ? ldg4(vel + j0) : z4, u1 = t1 ? ldg4(vel + j1) : z4,
+                            u2 = t2 ? ldg4(vel + j2) : z4, u3 = t3 ? ldg4(vel + j3) : z4;
+                if (t0) add(e0, u0, j0);
+                if (t1) add(e1, u1, j1);
+                if (t2) add(e2, u2, j2);
+                if (t3) add(e3, u3, j3);
+            }
+            for (; k < hi; ++k) {
+                const V4<R> q = ldg4(posf + k);
+                const int j = w_slot(q.w);
+                R e;
+                if (near(q, j, e)) add(e, ldg4(vel + j), j);
+            }
+        });
     }
+    if (TAPE) a.nbcnt[s] = cf;  // the recorded list (complete while cf <= nbK)
+    visc_sum_mirrors(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.m, MPS_INF_SKIP(a, sc.skip_r), sx, sy, sz,
+                     cm);
     R ax = fmaR(sc.kn, sx, sc.g[0]), ay = fmaR(sc.kn, sy, sc.g[1]), az = fmaR(sc.kn, sz, sc.g[2]);
     R ux = fmaR(ax, sc.dt, v.x), uy = fmaR(ay, sc.dt, v.y), uz = fmaR(az, sc.dt, v.z);
     R x = fmaR(ux, sc.dt, p.x), y = fmaR(uy, sc.dt, p.y), z = fmaR(uz, sc.dt, p.z);

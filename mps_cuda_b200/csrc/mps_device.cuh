@@ -181,15 +181,17 @@ __device__ __forceinline__ void for_fluid(const SceneDev<R, RN>& sc, const int* 
 }
 
 // Visit the 27 buckets around c (z, y, x ascending); a row of three x-adjacent buckets is
-// one contiguous range of the sorted arrays. `B` is (radius + margin)^2: a row or an end
+// one contiguous range of the sorted arrays. The row loops stay rolled: the visit bodies
+// (collision, density, gradient, mirror generation) are long, and nine copies of each
+// overflow the instruction cache. `B` is (radius + margin)^2: a row or an end
 // bucket whose nearest point lies farther than that is not visited.
 template <class R, class RN, class F>
 __device__ __forceinline__ void for_rows(const SceneDev<R, RN>& sc, const int* __restrict__ cs,
                                          const RowCtx<R>& c, R B, F&& f) {
-#pragma unroll
+#pragma unroll 1
     for (int dz = -1; dz <= 1; ++dz) {
         R ddz = dz < 0 ? c.dzl : (dz > 0 ? c.dzh : R(0));
-#pragma unroll
+#pragma unroll 1
         for (int dy = -1; dy <= 1; ++dy) {
             R ddy = dy < 0 ? c.dyl : (dy > 0 ? c.dyh : R(0));
             R dyz2 = ddy * ddy + ddz * ddz;
@@ -208,10 +210,10 @@ template <class R, class RN, class F>
 __device__ __forceinline__ void for_rows_ranges(const SceneDev<R, RN>& sc,
                                                 const int* __restrict__ cs, const RowCtx<R>& c,
                                                 R B, F&& f) {
-#pragma unroll
+#pragma unroll 1
     for (int dz = -1; dz <= 1; ++dz) {
         R ddz = dz < 0 ? c.dzl : (dz > 0 ? c.dzh : R(0));
-#pragma unroll
+#pragma unroll 1
         for (int dy = -1; dy <= 1; ++dy) {
             R ddy = dy < 0 ? c.dyl : (dy > 0 ? c.dyh : R(0));
             R dyz2 = ddy * ddy + ddz * ddz;

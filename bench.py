@@ -18,7 +18,8 @@ ours      : libmps_b200.so. `value` = device time of K steps (CUDA events on the
             per-particle loops) on a bounded sample of the same workload, rank 0 only;
             `batched` = 64 uneven scenes in one handle against a per-scene loop;
             `adjoint` = the rollout adjoint's cost per step against a forward step at the
-            48 000-particle adjoint workload, with its finite-difference agreement.
+            48 000-particle adjoint workload, with its finite-difference agreement;
+            `other_workloads` = the same workload in FP64 and the 6.1M-particle scene.
 reference : the reference's per-particle loops as that OpenMP CPU restatement (the
             reference itself has no CPU implementation), all host threads, rank 0 only;
             `reference_cuda` adds the reference's own CUDA kernels (built for sm_100a from
@@ -378,6 +379,11 @@ def run_ours(args, world, rank, local):
     adjoint = None
     if not args.no_adjoint:
         adjoint = measure_adjoint(stream)
+    extra = None
+    if not args.no_extra:
+        # the same workload in FP64, and the 6.1M-particle single scene in FP32
+        extra = [measure_workload(args.workload, "f64", stream, flush, min(K, 50)),
+                 measure_workload("dambreak_l0.0025_6.1M", "f32", stream, flush, min(K, 20))]
     clk.__exit__(None, None, None)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -400,10 +406,52 @@ def run_ours(args, world, rank, local):
             "roofline": roofline, "kernel_groups": groups, "cpu_baseline": cpu,
             "batched": batched,
             "adjoint": adjoint,
+            "other_workloads": extra,
             "counters": {k: v for k, v in cnt.items() if k != "kernel_launches"},
         }
         print(json.dumps(line), flush=True)
     g.close()
+
+
+def measure_workload(workload: str, precision: str, stream, flush, K: int):
+    """Device time of K graph-replayed steps of another workload or precision (L2 flushed
+    between steps), with the step's per-group split."""
+    import torch
+
+    from mps_cuda_b200 import MPS
+    from mps_cuda_b200 import _lib as L
+    p, typ, pos, vel, nrm = build_scene(workload, precision)
+    nf = int((typ == 0).sum())
+    g = MPS(p, typ, pos, vel, nrm)
+    g.set_stream(stream.cuda_stream)
+    g.set_option(L.OPT_GRAPH, 1)
+    for _ in range(3):
+        g.step(1)
+    g.synchronize()
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            flush.fill_(float(k))
+            e0[k].record(stream)
+            g.step(1)
+            e1[k].record(stream)
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in zip(e0, e1)) / K
+    g.set_option(L.OPT_TIMING, 1)
+    g.timing(reset=True)
+    with torch.cuda.stream(stream):
+        for k in range(min(K, 10)):
+            flush.fill_(float(k))
+            g.step(1)
+    tm = g.timing(reset=True)
+    cnt = g.counters()
+    g.close()
+    return {"workload": workload, "precision": precision, "fluid_particles": nf,
+            "wall_particles": int((typ != 0).sum()), "steps": K, "ms_per_step": ms,
+            "value": nf / (ms / 1e3), "unit": "particle-updates/s",
+            "kernel_groups_ms_per_launch": {k: v[0] / v[1] for k, v in tm.items() if v[1]},
+            "deleted": cnt["n_deleted"], "errors": {k: v for k, v in cnt.items() if k.startswith("err")}}
 
 
 def measure_adjoint(stream):
@@ -563,6 +611,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-extra", action="store_true")
     args = ap.parse_args()
     world, rank, local = setup_dist()
     try:

@@ -1,0 +1,76 @@
+"""A full run against the reference's own kernels: integral quantities within 0.5 %.
+
+The 6 000-particle dam break (l0 = 0.02 m, 1.0 x 0.2 x 0.8 m tank, dt = 2e-4 s) runs
+1 000 steps in FP64 through this library and through the reference's `class MPS` kernels
+(frsykzk/MPS_CUDA, built for sm_100a from its sources by oracle/ref_build.sh, FP64 variant).
+Every 100 steps the fluid centroid, the kinetic energy per unit mass (sum |v|^2 / 2), the
+surge front and the number of fluid particles alive are compared: each within 0.5 %
+relative of at least one of two runs of the reference (the reference does not reproduce
+itself exactly, see below).
+
+Two things bound what can be compared. The reference's corner mirror takes its plane point
+from the first Edge wall its linked list yields (kernel.cu:841-887), and the list order is
+run-to-run nondeterministic (kernel.cu:525-527): two runs of the reference itself differ by
+up to 1 % in kinetic energy during the start-up transient, all of it at particles near two
+or three walls, where a mirror moved by the choice changes the number density by O(1). This
+library fixes the choice (ascending id), so during that transient (the first 100 steps, when
+the jittered lattice settles) its kinetic energy differs by a few percent at the tank's edges
+while the particles away from the walls agree to the reference's own spread; the kinetic
+energy is compared from step 200 on. Later in the run the reference's two runs still differ
+by up to about 0.5 % in kinetic energy, hence the comparison with either run. The surge
+front is the mean x of the 1 % front-most particles: the single front-most particle differs
+by up to 0.4 % between two reference runs.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from mps_cuda_b200 import F64, MPS, configs, dambreak, dambreak_params, select_device
+from mps_cuda_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 5e-3
+
+
+def _integrals_of(st):
+    f = st["typ"] == L.FLD
+    p, v = st["pos"][:, f], st["vel"][:, f]
+    k = max(1, p.shape[1] // 100)
+    return {"cx": p[0].mean(), "cy": p[1].mean(), "cz": p[2].mean(),
+            "ke": 0.5 * float((v * v).sum()), "front": float(np.sort(p[0])[-k:].mean()),
+            "alive": int(f.sum())}
+
+
+def test_full_run_integrals_match_reference_kernels():
+    from oracle import refbind
+    if not refbind.available(1):
+        pytest.skip("the reference's kernels are not built here (oracle/ref_build.sh)")
+    select_device(0)
+    desc, dt, steps = configs.WORKLOADS["dambreak_l0.02_6k"]
+    sc = dambreak(desc)
+    p = dambreak_params(desc, dt=dt, precision=F64)
+    ours = MPS(p, sc["typ"], sc["pos"], sc["vel"], sc["nrm"])
+    refs = [refbind.Reference(p, sc["typ"], sc["pos"], sc["vel"], sc["nrm"]) for _ in range(2)]
+    spread = {}
+    try:
+        for k in range(steps // 100):
+            ours.step(100)
+            for r_ in refs:
+                r_.step(100)
+            a = _integrals_of(ours.state())
+            bs = [_integrals_of(r_.state()) for r_ in refs]
+            b = bs[0]
+            assert min(abs(a["alive"] - x["alive"]) for x in bs) <= max(2, b["alive"] // 1000)
+            for q in ("cx", "cy", "cz", "ke", "front"):
+                if q == "ke" and k < 1:
+                    continue  # the start-up transient (see the module docstring)
+                rel = min(abs(a[q] - x[q]) / max(abs(x[q]), 1e-12) for x in bs)
+                spread[q] = max(spread.get(q, 0.0), abs(bs[0][q] - bs[1][q]) / abs(bs[0][q]))
+                assert rel <= RTOL, (100 * (k + 1), q, a[q], [x[q] for x in bs])
+    finally:
+        ours.close()
+    # the run moved: the surge front advanced and the fluid gained kinetic energy
+    assert b["front"] > float(sc["pos"][0][sc["typ"] == L.FLD].max()) + 0.05
+    assert b["ke"] > 1.0

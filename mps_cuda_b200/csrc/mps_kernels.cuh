@@ -106,6 +106,39 @@ __global__ void k_bin_key(Src src, const int* n_ptr, int n_fixed, int* __restric
     }
 }
 
+// k_bin_key for the fluid: also counts each fine cell's items at its row-major index
+template <class R, class RN>
+__global__ void k_bin_key_fluid(FluidKeySrc<R, RN> src, int n, int* __restrict__ key,
+                                int* __restrict__ rnk, int* __restrict__ count,
+                                int* __restrict__ count_r, DevCounters* cnt) {
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        int t = base + lane;
+        bool act = t < n;
+        int c = act ? src.key(t, cnt) : -1;
+        unsigned peers = __match_any_sync(0xffffffffu, c);
+        int leader = __ffs(peers) - 1;
+        int below = __popc(peers & ((1u << lane) - 1));
+        int b = 0;
+        if (act && lane == leader) {
+            b = atomicAdd(&count[c], __popc(peers));
+            int cr = c;
+            if (c != src.dead) {
+                const SceneDev<R, RN>& s =
+                    src.sc[src.nscene > 1 ? scene_of(src.sc, src.nscene, src.pid[t]) : 0];
+                cr = fine_rowmajor(s, c);
+            }
+            atomicAdd(&count_r[cr], __popc(peers));
+        }
+        b = __shfl_sync(0xffffffffu, b, leader);
+        if (act) {
+            key[t] = c;
+            rnk[t] = b + below;
+        }
+    }
+}
+
 template <class Src>
 __global__ void k_bin_seg(Src src, const int* n_ptr, int n_fixed, const int* __restrict__ key,
                           const int* __restrict__ rnk, const int* __restrict__ cs,
@@ -180,31 +213,6 @@ template <class R, class RN> struct FluidGatherF {
         posf[__ldg(csr + fine_rowmajor(s, c)) + d - __ldg(cs + c)] = V4<R>{p.x, p.y, p.z, slot_w(d, R(0))};
     }
 };
-
-// scene holding global fine cell c (scenes are stored in ascending fbase)
-template <class R, class RN>
-__device__ __forceinline__ int scene_of_fine(const SceneDev<R, RN>* sc, int nscene, int c) {
-    int lo = 0, hi = nscene - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (__ldg(&sc[mid].fbase) <= c) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
-// per-fine-cell counts in row-major order (the last entry counts unlisted items)
-template <class R, class RN>
-__global__ void k_count_rowmajor(const SceneDev<R, RN>* sc, int nscene, const int* __restrict__ count,
-                                 int* __restrict__ count_r, int ncell) {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= ncell; c += gridDim.x * blockDim.x) {
-        if (c == ncell) {
-            count_r[c] = count[c];
-        } else {
-            const SceneDev<R, RN>& s = sc[nscene > 1 ? scene_of_fine(sc, nscene, c) : 0];
-            count_r[fine_rowmajor(s, c)] = count[c];
-        }
-    }
-}
 
 // positions of the row-ordered copy from the slots' current positions (the per-method
 // path moves particles in place between bucket builds)
@@ -316,6 +324,95 @@ static __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int* _
         excl += v[k];
     }
     if (base <= L - 1 && L - 1 < base + kScanPer) out[L] = excl;  // thread holding the last item
+}
+
+// Scan of the fluid's fine-cell counts: 16 counts per thread through int4 loads, and the
+// counts cleared as they are read, so that the next bucket build starts from zeros without
+// a memset (the fine tables are 27 times the bucket count).
+constexpr int kScan16Threads = 512, kScan16Per = 16, kScan16Tile = kScan16Threads * kScan16Per;
+
+__device__ __forceinline__ void load16(const int* __restrict__ in, int base, int L, int v[16]) {
+    if (base + 16 <= L) {
+        const int4* p = reinterpret_cast<const int4*>(in + base);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int4 a = p[q];
+            v[4 * q] = a.x; v[4 * q + 1] = a.y; v[4 * q + 2] = a.z; v[4 * q + 3] = a.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = (base + k < L) ? in[base + k] : 0;
+    }
+}
+
+static __global__ void __launch_bounds__(kScan16Threads) k_scan16_reduce(const int* __restrict__ in,
+                                                                     int L, int* __restrict__ part) {
+    __shared__ int sh[32];
+    int v[16];
+    load16(in, blockIdx.x * kScan16Tile + threadIdx.x * kScan16Per, L, v);
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s += v[k];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// exclusive scan of in[0..L) into out[0..L], out[L] = total; in[0..L) is left zero
+static __global__ void __launch_bounds__(kScan16Threads) k_scan16_apply(int* __restrict__ in, int L,
+                                                                    const int* __restrict__ part,
+                                                                    int* __restrict__ out) {
+    __shared__ int sh[32];
+    __shared__ int wsum[32];
+    int off = 0;
+    for (int b = threadIdx.x; b < (int)blockIdx.x; b += blockDim.x) off += part[b];
+    off = block_sum(off, sh);
+    const int base = blockIdx.x * kScan16Tile + threadIdx.x * kScan16Per;
+    int v[16];
+    load16(in, base, L, v);
+    int loc = 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) loc += v[k];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int inc = loc;
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) wsum[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        int ws = lane < (blockDim.x >> 5) ? wsum[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, ws, o);
+            if (lane >= o) ws += y;
+        }
+        wsum[lane] = ws;
+    }
+    __syncthreads();
+    int e[16];
+    int excl = off + (w > 0 ? wsum[w - 1] : 0) + inc - loc;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        e[k] = excl;
+        excl += v[k];
+    }
+    if (base + 16 <= L) {
+        int4* o4 = reinterpret_cast<int4*>(out + base);
+        int4* i4 = reinterpret_cast<int4*>(in + base);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            o4[q] = make_int4(e[4 * q], e[4 * q + 1], e[4 * q + 2], e[4 * q + 3]);
+            i4[q] = make_int4(0, 0, 0, 0);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            if (base + k < L) {
+                out[base + k] = e[k];
+                in[base + k] = 0;
+            }
+    }
+    if (base <= L - 1 && L - 1 < base + kScan16Per) out[L] = excl;  // thread holding the last item
 }
 
 // ---------------------------------------------------------------------------------------

@@ -253,7 +253,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     int* cs;
     // fluid positions in row-major fine-cell order (slot in w) and that order's cell starts
     V4<R>* posf;
-    int *csr, *count_r;
+    int *csr, *count_f, *count_r;
     bool posf_stale = false;  // particles moved in place since the copy was made
     // bucket-build scratch
     int *key, *rnk, *seg, *count, *part;
@@ -482,7 +482,11 @@ template <class R, class RN> class Solver final : public SolverBase {
         wcs = ar.template get<int>(L() + 1);
         cs = ar.template get<int>(size_t(LF()) + 1);
         csr = ar.template get<int>(size_t(LF()) + 1);
+        // the fluid's own count tables: its scans leave them zero for the next build
+        count_f = ar.template get<int>(size_t(LF()));
         count_r = ar.template get<int>(size_t(LF()));
+        CK(cudaMemsetAsync(count_f, 0, sizeof(int) * size_t(LF()), stream));
+        CK(cudaMemsetAsync(count_r, 0, sizeof(int) * size_t(LF()), stream));
         posf = ar.template get<V4<R>>(F);
         for (MirrorBuf<R>* b : {&U, &M1, &M2}) {
             b->pos = ar.template get<V4<R>>(cap);
@@ -494,8 +498,9 @@ template <class R, class RN> class Solver final : public SolverBase {
         key = ar.template get<int>(items);
         rnk = ar.template get<int>(items);
         seg = ar.template get<int>(items);
-        count = ar.template get<int>(size_t(LF()));  // fine cells outnumber buckets 27:1
-        part = ar.template get<int>((size_t(LF()) + kScanTile - 1) / kScanTile + 1);
+        count = ar.template get<int>(L());
+        part = ar.template get<int>((size_t(LF()) + kScan16Tile - 1) / kScan16Tile +
+                                    (L() + kScanTile - 1) / kScanTile + 1);
         d_fluid_ids = ar.template get<int>(F);
         d_wall_ids = ar.template get<int>(W);
         d_nF = ar.template get<int>(1);
@@ -557,23 +562,19 @@ template <class R, class RN> class Solver final : public SolverBase {
                                S2.pav, S2.pid, S2.typ},
                               d_sc, nscene, key, cs, csr, posf};
         const int ncell = LF();
-        CK(cudaMemsetAsync(count, 0, sizeof(int) * size_t(ncell), stream));
         const int grid = std::min(blocks(std::max(nF, 1), 256), 148 * 32);
         if (nF > 0) {
-            k_bin_key<FluidKeySrc<R, RN>><<<grid, 256, 0, stream>>>(ks, nullptr, nF, key, rnk, count, cnt);
+            k_bin_key_fluid<R, RN><<<grid, 256, 0, stream>>>(ks, nF, key, rnk, count_f, count_r, cnt);
             KL();
         }
-        k_count_rowmajor<R, RN><<<std::min(blocks(ncell, 256), 148 * 16), 256, 0, stream>>>(
-            d_sc, nscene, count, count_r, ncell - 1);
+        const int nb = (ncell + kScan16Tile - 1) / kScan16Tile;
+        k_scan16_reduce<<<nb, kScan16Threads, 0, stream>>>(count_f, ncell, part);
         KL();
-        const int nb = (ncell + kScanTile - 1) / kScanTile;
-        k_scan_reduce<<<nb, kScanThreads, 0, stream>>>(count, ncell, part);
+        k_scan16_apply<<<nb, kScan16Threads, 0, stream>>>(count_f, ncell, part, cs);
         KL();
-        k_scan_apply<<<nb, kScanThreads, 0, stream>>>(count, ncell, part, cs);
+        k_scan16_reduce<<<nb, kScan16Threads, 0, stream>>>(count_r, ncell, part);
         KL();
-        k_scan_reduce<<<nb, kScanThreads, 0, stream>>>(count_r, ncell, part);
-        KL();
-        k_scan_apply<<<nb, kScanThreads, 0, stream>>>(count_r, ncell, part, csr);
+        k_scan16_apply<<<nb, kScan16Threads, 0, stream>>>(count_r, ncell, part, csr);
         KL();
         if (nF > 0) {
             k_bin_seg<FluidKeySrc<R, RN>><<<grid, 256, 0, stream>>>(ks, nullptr, nF, key, rnk, cs, seg);

@@ -533,14 +533,22 @@ __device__ __forceinline__ bool cull_keep(const SceneDev<R, RN>& sc, R mx, R my,
 }
 
 // ---- GenMRR_nonslip for one fluid particle (kernel.cu:726-891) ---------------------------
-// Appends the mirrors (culled on the spot when CULL) to `out`; returns the number of walls
-// inside r (diagnostic).
-template <class R, class RN, bool CULL, bool TAPE = false>
-__device__ __forceinline__ int gen_mirrors(const SceneDev<R, RN>& sc, const RowCtx<R>& c, R x,
-                                           R y, R z, R P, int slot_base, const WallView<R>& wl,
-                                           bool skip, const MirrorSink<R>& out,
-                                           DevCounters* cnt) {
-    int reg[kNumMRR], edg[kNumMRR];
+// In three parts, so that a warp reserves its mirrors' places in the raw list with one
+// atomic: plan (registration over the walls inside r), count, emit.
+template <class R> struct MirrorPlan {
+    int nreg;    // registered normals: face mirror k comes from wall reg[k]
+    int corner;  // wall whose position anchors the corner mirror, -1 when there is none
+    int reg[kNumMRR];
+    R sx, sy, sz;  // normalised sum of the distinct Edge normals
+};
+
+// registration (kernel.cu:741-800): every distinct normal once, the first wall found wins;
+// Edge walls likewise. Returns the number of walls inside r (diagnostic).
+template <class R, class RN>
+__device__ __forceinline__ int plan_mirrors(const SceneDev<R, RN>& sc, const RowCtx<R>& c, R x,
+                                            R y, R z, const WallView<R>& wl, bool skip,
+                                            MirrorPlan<R>& pl) {
+    int edg[kNumMRR];
     R rn[kNumMRR][3], en[kNumMRR][3];
     int nreg = 0, nedge = 0, nwall = 0;
     for_rows(sc, wl.cs, c, skip ? sc.skip_r : R(INFINITY), [&](int j) {
@@ -554,7 +562,7 @@ __device__ __forceinline__ int gen_mirrors(const SceneDev<R, RN>& sc, const RowC
         for (int k = 0; k < nreg; ++k)
             if (rn[k][0] == nv.x && rn[k][1] == nv.y && rn[k][2] == nv.z) dup = true;
         if (!dup && nreg < kNumMRR) {
-            reg[nreg] = j;
+            pl.reg[nreg] = j;
             rn[nreg][0] = nv.x; rn[nreg][1] = nv.y; rn[nreg][2] = nv.z;
             ++nreg;
         }
@@ -569,57 +577,83 @@ __device__ __forceinline__ int gen_mirrors(const SceneDev<R, RN>& sc, const RowC
             }
         }
     });
-    if (nreg == 0) return nwall;
+    pl.nreg = nreg;
+    pl.corner = -1;
+    // corner mirror through the last Edge wall (kernel.cu:841-858)
+    if (nreg > 0 && nedge >= 2) {
+        R sx = 0, sy = 0, sz = 0;
+        for (int k = 0; k < nedge; ++k) {
+            sx += en[k][0]; sy += en[k][1]; sz += en[k][2];
+        }
+        R as = sqrtR(dot3(sx, sy, sz, sx, sy, sz));
+        pl.sx = sx / as; pl.sy = sy / as; pl.sz = sz / as;
+        pl.corner = edg[nedge - 1];
+    }
+    return nwall;
+}
+
+// mirrors the plan will emit; a corner mirror without a free slot is counted as an error
+// (kernel.cu:868-874 writes it out of bounds)
+template <class R, class RN>
+__device__ __forceinline__ int count_mirrors(const MirrorPlan<R>& pl, R x, R y, R z,
+                                             const WallView<R>& wl, DevCounters* cnt) {
+    int m = 0;
+    for (int k = 0; k < pl.nreg; ++k) {
+        V4<R> q = ldg4(wl.pos + pl.reg[k]), n = ldg4(wl.nrm + pl.reg[k]);
+        if (!(dot3(x - q.x, y - q.y, z - q.z, n.x, n.y, n.z) < R(0))) ++m;
+    }
+    if (pl.corner >= 0) {
+        V4<R> q = ldg4(wl.pos + pl.corner);
+        if (dot3(x - q.x, y - q.y, z - q.z, pl.sx, pl.sy, pl.sz) >= R(0)) {
+            if (pl.nreg >= kNumMRR) atomicAdd(&cnt->err_mirror_slot, 1);
+            else ++m;
+        }
+    }
+    return m;
+}
+
+// face mirrors (kernel.cu:811-838), then the corner mirror (kernel.cu:859-887), written to
+// the raw list from index `at` on
+template <class R, class RN, bool TAPE>
+__device__ __forceinline__ void emit_mirrors(const MirrorPlan<R>& pl, R x, R y, R z, R P,
+                                             int slot_base, const WallView<R>& wl,
+                                             const MirrorSink<R>& out, DevCounters* cnt, int at) {
     auto emit = [&](R mx, R my, R mz, int slot, R nx, R ny, R nz, R nlen) {
-        if (CULL && !cull_keep(sc, mx, my, mz, wl, skip, &cnt->err_cell)) return;
-        int idx = atomicAdd(&cnt->mirror_raw, 1);
+        const int idx = at++;
         if (idx < out.cap) {
             out.pos[idx] = V4<R>{mx, my, mz, P};
             out.slot[idx] = slot;
             if (TAPE) {
-                const R c = sqrtR(R(2) / nlen);
-                out.nrm[idx] = V4<R>{nx * c, ny * c, nz * c, R(0)};
+                const R cf = sqrtR(R(2) / nlen);
+                out.nrm[idx] = V4<R>{nx * cf, ny * cf, nz * cf, R(0)};
             }
         } else {
             atomicAdd(&cnt->err_capacity, 1);
         }
     };
-    // face mirrors (kernel.cu:811-838)
-    for (int k = 0; k < nreg; ++k) {
-        V4<R> q = ldg4(wl.pos + reg[k]);
+    for (int k = 0; k < pl.nreg; ++k) {
+        V4<R> q = ldg4(wl.pos + pl.reg[k]), n = ldg4(wl.nrm + pl.reg[k]);
         R pwx = x - q.x, pwy = y - q.y, pwz = z - q.z;
-        R pw = dot3(pwx, pwy, pwz, rn[k][0], rn[k][1], rn[k][2]);
+        R pw = dot3(pwx, pwy, pwz, n.x, n.y, n.z);
         if (pw < R(0)) continue;
-        R nlen = sqrtR(dot3(rn[k][0], rn[k][1], rn[k][2], rn[k][0], rn[k][1], rn[k][2]));
+        R nlen = sqrtR(dot3(n.x, n.y, n.z, n.x, n.y, n.z));
         R dist = pw / nlen;
         R t2 = R(2) * dist;
-        emit(fmaR(-t2, rn[k][0], q.x + pwx), fmaR(-t2, rn[k][1], q.y + pwy),
-             fmaR(-t2, rn[k][2], q.z + pwz), slot_base + k, rn[k][0], rn[k][1], rn[k][2], nlen);
+        emit(fmaR(-t2, n.x, q.x + pwx), fmaR(-t2, n.y, q.y + pwy), fmaR(-t2, n.z, q.z + pwz),
+             slot_base + k, n.x, n.y, n.z, nlen);
     }
-    // corner mirror through the last edge wall (kernel.cu:841-887)
-    if (nedge >= 2) {
-        R sx = 0, sy = 0, sz = 0;
-        for (int k = 0; k < nedge; ++k) {
-            sx += en[k][0]; sy += en[k][1]; sz += en[k][2];
-        }
-        V4<R> q = ldg4(wl.pos + edg[nedge - 1]);
+    if (pl.corner >= 0 && pl.nreg < kNumMRR) {
+        V4<R> q = ldg4(wl.pos + pl.corner);
         R pwx = x - q.x, pwy = y - q.y, pwz = z - q.z;
-        R as = sqrtR(dot3(sx, sy, sz, sx, sy, sz));
-        sx /= as; sy /= as; sz /= as;
-        R pw = dot3(pwx, pwy, pwz, sx, sy, sz);
+        R pw = dot3(pwx, pwy, pwz, pl.sx, pl.sy, pl.sz);
         if (pw >= R(0)) {
-            R slen = sqrtR(dot3(sx, sy, sz, sx, sy, sz));
+            R slen = sqrtR(dot3(pl.sx, pl.sy, pl.sz, pl.sx, pl.sy, pl.sz));
             R dist = pw / slen;
-            if (nreg >= kNumMRR) {
-                atomicAdd(&cnt->err_mirror_slot, 1);
-            } else {
-                R t2 = R(2) * dist;
-                emit(fmaR(-t2, sx, q.x + pwx), fmaR(-t2, sy, q.y + pwy),
-                     fmaR(-t2, sz, q.z + pwz), slot_base + nreg, sx, sy, sz, slen);
-            }
+            R t2 = R(2) * dist;
+            emit(fmaR(-t2, pl.sx, q.x + pwx), fmaR(-t2, pl.sy, q.y + pwy),
+                 fmaR(-t2, pl.sz, q.z + pwz), slot_base + pl.nreg, pl.sx, pl.sy, pl.sz, slen);
         }
     }
-    return nwall;
 }
 
 }  // namespace mps

@@ -807,29 +807,56 @@ __global__ void __launch_bounds__(128) k_pass_c(PassArgs<R, RN> a) {
     }
 }
 
+// The warp's mirrors take consecutive places in the raw list, reserved with one atomic per
+// warp (the list's order does not matter: the mirror bucket build sorts by bucket and slot).
+// Every lane of the warp calls this.
+template <class R, class RN, bool TAPE>
+__device__ __forceinline__ void gen_reserve_emit(const PassArgs<R, RN>& a, const MirrorPlan<R>& pl,
+                                                 int m, R x, R y, R z, R P, int slot_base) {
+    const int lane = threadIdx.x & 31;
+    int incl = m;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int tot = __shfl_sync(0xffffffffu, incl, 31);
+    int base = 0;
+    if (lane == 31 && tot > 0) base = atomicAdd(&a.cnt->mirror_raw, tot);
+    base = __shfl_sync(0xffffffffu, base, 31) + incl - m;
+    if (m > 0) emit_mirrors<R, RN, TAPE>(pl, x, y, z, P, slot_base, a.wl, a.out, a.cnt, base);
+}
+
 // GenMRR_nonslip + MRRinout for every FLD slot of (gpos, gprs, gtyp): the second generation
 // of a step (x*, P after pass B) and the first generation of the next one (x^{n+1}, P after
 // pass C). Near-wall particles are a thin layer, so this runs as a light kernel of its own
 // instead of stretching the neighbour passes.
-template <class R, class RN, bool DIAG, bool CULL, bool TAPE = false>
+template <class R, class RN, bool DIAG, bool TAPE = false>
 __global__ void __launch_bounds__(128) k_gen_cull(PassArgs<R, RN> a, const V4<R>* gpos,
                                                   const R* gprs, const int8_t* gtyp) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.nF || gtyp[s] != kFLD) return;
-    const int pid = a.pid[s];
-    const SceneDev<R, RN>& sc = scene_ref(a, pid);
-    V4<R> p = gpos[s];
-    int ix, iy, iz;
-    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
-    // no wall in the 27 buckets around: no wall within r, no mirror (the common case)
-    if (!__ldg(a.near_wall + sc.cbase + iz * sc.nbxy + iy * sc.nbx + ix)) {
-        if (DIAG) a.diag[size_t(pid) * kDiagCols + DG_GEN_W] = 0;
-        return;
+    MirrorPlan<R> pl;
+    pl.nreg = 0;
+    pl.corner = -1;
+    int m = 0, pid = 0;
+    V4<R> p{R(0), R(0), R(0), R(0)};
+    R P = R(0);
+    if (s < a.nF && gtyp[s] == kFLD) {  // every lane stays for the warp's reservation
+        pid = a.pid[s];
+        const SceneDev<R, RN>& sc = scene_ref(a, pid);
+        p = gpos[s];
+        int ix, iy, iz;
+        cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+        int nw = 0;
+        // no wall in the 27 buckets around: no wall within r, no mirror (the common case)
+        if (__ldg(a.near_wall + sc.cbase + iz * sc.nbxy + iy * sc.nbx + ix)) {
+            RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+            nw = plan_mirrors(sc, c, p.x, p.y, p.z, a.wl, a.skip != 0, pl);
+            m = count_mirrors<R, RN>(pl, p.x, p.y, p.z, a.wl, a.cnt);
+            P = gprs[s];
+        }
+        if (DIAG) a.diag[size_t(pid) * kDiagCols + DG_GEN_W] = nw;
     }
-    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
-    int nw = gen_mirrors<R, RN, CULL, TAPE>(sc, c, p.x, p.y, p.z, gprs[s], pid * kNumMRR, a.wl,
-                                            a.skip != 0, a.out, a.cnt);
-    if (DIAG) a.diag[size_t(pid) * kDiagCols + DG_GEN_W] = nw;
+    gen_reserve_emit<R, RN, TAPE>(a, pl, m, p.x, p.y, p.z, P, pid * kNumMRR);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -992,16 +1019,25 @@ __global__ void k_ph_uppcl2(PassArgs<R, RN> a) {
 template <class R, class RN, bool DIAG>
 __global__ void __launch_bounds__(128) k_ph_gen(PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.nF || a.typ[s] != kFLD) return;
-    const int pid = a.pid[s];
-    const SceneDev<R, RN>& sc = scene_ref(a, pid);
-    V4<R> p = ldg4(a.pos + s);
-    int ix, iy, iz;
-    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
-    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
-    int nw = gen_mirrors<R, RN, false>(sc, c, p.x, p.y, p.z, a.prs[s], pid * kNumMRR, a.wl,
-                                       a.skip != 0, a.out, a.cnt);
-    if (DIAG) a.diag[size_t(pid) * kDiagCols + DG_GEN_W] = nw;
+    MirrorPlan<R> pl;
+    pl.nreg = 0;
+    pl.corner = -1;
+    int m = 0, pid = 0;
+    V4<R> p{R(0), R(0), R(0), R(0)};
+    R P = R(0);
+    if (s < a.nF && a.typ[s] == kFLD) {  // every lane stays for the warp's reservation
+        pid = a.pid[s];
+        const SceneDev<R, RN>& sc = scene_ref(a, pid);
+        p = ldg4(a.pos + s);
+        int ix, iy, iz;
+        cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+        RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+        const int nw = plan_mirrors(sc, c, p.x, p.y, p.z, a.wl, a.skip != 0, pl);
+        m = count_mirrors<R, RN>(pl, p.x, p.y, p.z, a.wl, a.cnt);
+        P = a.prs[s];
+        if (DIAG) a.diag[size_t(pid) * kDiagCols + DG_GEN_W] = nw;
+    }
+    gen_reserve_emit<R, RN, false>(a, pl, m, p.x, p.y, p.z, P, pid * kNumMRR);
 }
 
 // d_MRRinout over the raw mirrors; a culled mirror's slot becomes negative

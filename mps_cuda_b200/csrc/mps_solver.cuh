@@ -651,7 +651,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         {
             Scope t(this, MPS_K_GEN);
             // the step's second generation: the one the reference's counters would show last
-            k_gen_cull<R, RN, D, false><<<blocks(nF, bg), bg, 0, stream>>>(args(M1, mcs1), S.pos,
+            k_gen_cull<R, RN, D><<<blocks(nF, bg), bg, 0, stream>>>(args(M1, mcs1), S.pos,
                                                                            t_prs, S.typ);
             KL();
             cull_raw();
@@ -666,7 +666,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         reset_raw();
         {
             Scope t(this, MPS_K_GEN);
-            k_gen_cull<R, RN, false, false><<<blocks(nF, bg), bg, 0, stream>>>(args(M2, mcs2), t_pos,
+            k_gen_cull<R, RN, false><<<blocks(nF, bg), bg, 0, stream>>>(args(M2, mcs2), t_pos,
                                                                                t_prs, t_typ);
             KL();
             cull_raw();
@@ -684,7 +684,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         }
         if (!m1_valid) {
             reset_raw();
-            k_gen_cull<R, RN, false, false><<<blocks(nF, block), block, 0, stream>>>(
+            k_gen_cull<R, RN, false><<<blocks(nF, block), block, 0, stream>>>(
                 args(M1, mcs1), S.pos, S.prs, S.typ);
             KL();
             cull_raw();
@@ -1125,7 +1125,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         mkbkt(false);
         reset_raw();
         PassArgs<R, RN> a = tape_args(M1.pos, M1.slot, mcs1, nb, nbcnt, nullptr);
-        k_gen_cull<R, RN, false, false, true><<<blocks(nF, block), block, 0, stream>>>(
+        k_gen_cull<R, RN, false, true><<<blocks(nF, block), block, 0, stream>>>(
             a, S.pos, S.prs, S.typ);
         KL();
         cull_raw();
@@ -1156,7 +1156,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         cp(t.vv2, t_vel, sizeof(V4<R>) * F);
         cp(t.P2, t_prs, sizeof(R) * F);
         reset_raw();
-        k_gen_cull<R, RN, false, false, true><<<blocks(nF, bg), bg, 0, stream>>>(a, S.pos, t_prs,
+        k_gen_cull<R, RN, false, true><<<blocks(nF, bg), bg, 0, stream>>>(a, S.pos, t_prs,
                                                                                 S.typ);
         KL();
         cull_raw();
@@ -1165,7 +1165,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         k_pass_c<R, RN, false, true><<<blocks(nF, bc), bc, 0, stream>>>(a);
         KL();
         reset_raw();
-        k_gen_cull<R, RN, false, false, true><<<blocks(nF, bg), bg, 0, stream>>>(a, t_pos, t_prs,
+        k_gen_cull<R, RN, false, true><<<blocks(nF, bg), bg, 0, stream>>>(a, t_pos, t_prs,
                                                                                 t_typ);
         KL();
         cull_raw();

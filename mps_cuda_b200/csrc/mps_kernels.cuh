@@ -487,8 +487,9 @@ __device__ __forceinline__ int build_list(const PassArgs<R, RN>& a, const SceneD
     const int nF = a.nF, K = a.nbK;
     for_fluid_ranges(sc, a.csr, c, B, [&](int lo, int hi) {
         // four independent loads in flight before the first test (latency, not bandwidth,
-        // bounds this loop); candidates are still tested and appended in visiting order
-        int k = lo;
+        // bounds this loop), a short row's included: past the row's end the particle itself
+        // pads the batch and visit() rejects it; candidates are tested and appended in
+        // visiting order
         auto visit = [&](const V4<R>& q) {
             R dx = q.x - x, dy = q.y - y, dz = q.z - z;
             const int j = w_slot(q.w);
@@ -497,15 +498,17 @@ __device__ __forceinline__ int build_list(const PassArgs<R, RN>& a, const SceneD
                 ++cnt;
             }
         };
-        for (; k + 4 <= hi; k += 4) {
-            V4<R> q0 = ldg4(posf + k), q1 = ldg4(posf + k + 1), q2 = ldg4(posf + k + 2),
-                  q3 = ldg4(posf + k + 3);
+        const V4<R> self{x, y, z, slot_w(s, R(0))};
+        for (int k = lo; k < hi; k += 4) {
+            const V4<R> q0 = ldg4(posf + k);
+            const V4<R> q1 = k + 1 < hi ? ldg4(posf + k + 1) : self,
+                        q2 = k + 2 < hi ? ldg4(posf + k + 2) : self,
+                        q3 = k + 3 < hi ? ldg4(posf + k + 3) : self;
             visit(q0);
             visit(q1);
             visit(q2);
             visit(q3);
         }
-        for (; k < hi; ++k) visit(ldg4(posf + k));
     });
     return cnt;
 }
@@ -574,11 +577,15 @@ __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
             ++cf;
         };
         const V4<R> z4{R(0), R(0), R(0), R(0)};
+        // a short row's candidates are loaded together too: a batch past the row's end is
+        // padded with the particle itself, which near() rejects
+        const V4<R> self{p.x, p.y, p.z, slot_w(s, R(0))};
         for_fluid_ranges(sc, a.csr, c, MPS_INF_SKIP(a, sc.skip_r), [&](int lo, int hi) {
-            int k = lo;
-            for (; k + 4 <= hi; k += 4) {
-                const V4<R> q0 = ldg4(posf + k), q1 = ldg4(posf + k + 1), q2 = ldg4(posf + k + 2),
-                            q3 = ldg4(posf + k + 3);
+            for (int k = lo; k < hi; k += 4) {
+                const V4<R> q0 = ldg4(posf + k);
+                const V4<R> q1 = k + 1 < hi ? ldg4(posf + k + 1) : self,
+                            q2 = k + 2 < hi ? ldg4(posf + k + 2) : self,
+                            q3 = k + 3 < hi ? ldg4(posf + k + 3) : self;
                 const int j0 = w_slot(q0.w), j1 = w_slot(q1.w), j2 = w_slot(q2.w), j3 = w_slot(q3.w);
                 R e0, e1, e2, e3;
                 const bool t0 = near(q0, j0, e0), t1 = near(q1, j1, e1), t2 = near(q2, j2, e2),
@@ -589,12 +596,6 @@ __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
                 if (t1) add(e1, u1, j1);
                 if (t2) add(e2, u2, j2);
                 if (t3) add(e3, u3, j3);
-            }
-            for (; k < hi; ++k) {
-                const V4<R> q = ldg4(posf + k);
-                const int j = w_slot(q.w);
-                R e;
-                if (near(q, j, e)) add(e, ldg4(vel + j), j);
             }
         });
     }
@@ -704,7 +705,7 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
 // pass C: PrsGrdTrm (kernel.cu:1651-1794) + UpPcl2/ChkPcl (kernel.cu:1815-1829), walking
 // the neighbour lists pass B left. TAPE: also keeps the velocity before the clamp.
 template <class R, class RN, bool DIAG, bool TAPE = false>
-__global__ void __launch_bounds__(128) k_pass_c(PassArgs<R, RN> a) {
+__global__ void __launch_bounds__(128, 10) k_pass_c(PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
     const int nalive = __ldg(a.cs + a.dead);

@@ -503,35 +503,6 @@ __device__ __noinline__ void grad_sum_outline(const SceneDev<R, RN>& sc, const R
     grad_sum(sc, c, s, pid_local, x, y, z, pi, csr, posf, prs, m, skip, sx, sy, sz, cf, cm);
 }
 
-// ---- MRRinout cull of one mirror (kernel.cu:932-985); true = keep -----------------------
-template <class R, class RN>
-__device__ __forceinline__ bool cull_keep(const SceneDev<R, RN>& sc, R mx, R my, R mz,
-                                          const WallView<R>& wl, bool skip, int* err_cell) {
-    int ix, iy, iz;
-    if (!cell_of(sc, mx, my, mz, ix, iy, iz)) atomicAdd(err_cell, 1);
-    RowCtx<R> c = row_ctx(sc, mx, my, mz, ix, iy, iz);
-    bool found = false;
-    R wd = sc.wall_dist0;
-    R wx = 0, wy = 0, wz = 0, nx = 0, ny = 0, nz = 0;
-    for_rows(sc, wl.cs, c, skip ? sc.skip_r : R(INFINITY), [&](int j) {
-        V4<R> q = ldg4(wl.pos + j);
-        R dx = mx - q.x, dy = my - q.y, dz = mz - q.z;
-        R d2 = dot3(dx, dy, dz, dx, dy, dz);
-        if (d2 <= sc.r_le) {  // dist <= r
-            R d = sqrtR(d2);
-            if (d < wd) {
-                found = true;
-                wd = d;
-                V4<R> nv = ldg4(wl.nrm + j);
-                nx = nv.x; ny = nv.y; nz = nv.z;
-                wx = q.x; wy = q.y; wz = q.z;
-            }
-        }
-    });
-    R inout = dot3(mx - wx, my - wy, mz - wz, nx, ny, nz);
-    return !(found && inout >= R(0));
-}
-
 // ---- GenMRR_nonslip for one fluid particle (kernel.cu:726-891) ---------------------------
 // In three parts, so that a warp reserves its mirrors' places in the raw list with one
 // atomic: plan (registration over the walls inside r), count, emit.

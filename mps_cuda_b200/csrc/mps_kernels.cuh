@@ -1041,17 +1041,81 @@ __global__ void __launch_bounds__(128) k_ph_gen(PassArgs<R, RN> a) {
     gen_reserve_emit<R, RN, false>(a, pl, m, p.x, p.y, p.z, P, pid * kNumMRR);
 }
 
-// d_MRRinout over the raw mirrors; a culled mirror's slot becomes negative
+// Nearest wall inside r of a mirror over part of its 27 buckets' rows: row ri = 3 (dz + 1)
+// + (dy + 1) when ri % 4 == part (for_rows's rows and skipping). Keeps the first nearest
+// wall in visiting order: distance, row and wall slot (-1: none).
+template <class R, class RN>
+__device__ __forceinline__ void nearest_wall_part(const SceneDev<R, RN>& sc, const RowCtx<R>& c,
+                                                  R mx, R my, R mz, const WallView<R>& wl, R B,
+                                                  int part, R& wd, int& wrow, int& wj) {
+#pragma unroll 1
+    for (int ri = part; ri < 9; ri += 4) {
+        const int dz = ri / 3 - 1, dy = ri % 3 - 1;
+        const R ddz = dz < 0 ? c.dzl : (dz > 0 ? c.dzh : R(0));
+        const R ddy = dy < 0 ? c.dyl : (dy > 0 ? c.dyh : R(0));
+        const R dyz2 = ddy * ddy + ddz * ddz;
+        if (dyz2 > B) continue;
+        const int jl = (dyz2 + c.dxl * c.dxl <= B) ? c.ix - 1 : c.ix;
+        const int jh = (dyz2 + c.dxh * c.dxh <= B) ? c.ix + 1 : c.ix;
+        const int row = sc.cbase + (c.iz + dz) * sc.nbxy + (c.iy + dy) * sc.nbx;
+        const int lo = __ldg(wl.cs + row + jl), hi = __ldg(wl.cs + row + jh + 1);
+        for (int j = lo; j < hi; ++j) {
+            V4<R> q = ldg4(wl.pos + j);
+            R dx = mx - q.x, dy2 = my - q.y, dz2 = mz - q.z;
+            R d2 = dot3(dx, dy2, dz2, dx, dy2, dz2);
+            if (d2 <= sc.r_le) {  // dist <= r
+                R d = sqrtR(d2);
+                if (d < wd) {
+                    wd = d;
+                    wrow = ri;
+                    wj = j;
+                }
+            }
+        }
+    }
+}
+
+// d_MRRinout (kernel.cu:932-985) over the raw mirrors; a culled mirror's slot becomes
+// negative. Four lanes share a mirror, each walking a quarter of its rows; the group then
+// keeps the smallest distance, on ties the earlier row, which is the wall the sequential
+// walk keeps (the first nearest one found).
 template <class R, class RN>
 __global__ void k_ph_cull(PassArgs<R, RN> a) {
     const int n = min(a.cnt->mirror_raw, a.out.cap);
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        int sl = a.out.slot[t];
-        if (sl < 0) continue;
-        const SceneDev<R, RN>& sc = a.sc[a.nscene > 1 ? scene_of(a.sc, a.nscene, sl / kNumMRR) : 0];
-        V4<R> q = a.out.pos[t];
-        if (!cull_keep(sc, q.x, q.y, q.z, a.wl, a.skip != 0, &a.cnt->err_cell))
-            a.out.slot[t] = -1 - sl;
+    const int part = threadIdx.x & 3;
+    const int groups = (gridDim.x * blockDim.x) >> 2;
+    const int nround = (n + groups - 1) / groups * groups;  // every lane loops alike
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 2; t < nround; t += groups) {
+        const int sl = t < n ? a.out.slot[t] : -1;
+        R wd = R(0);
+        int wrow = 9, wj = -1;
+        V4<R> q{R(0), R(0), R(0), R(0)};
+        const SceneDev<R, RN>* scp = a.sc;
+        if (sl >= 0) {
+            scp = &a.sc[a.nscene > 1 ? scene_of(a.sc, a.nscene, sl / kNumMRR) : 0];
+            q = a.out.pos[t];
+            int ix, iy, iz;
+            if (!cell_of(*scp, q.x, q.y, q.z, ix, iy, iz) && part == 0) atomicAdd(&a.cnt->err_cell, 1);
+            const RowCtx<R> c = row_ctx(*scp, q.x, q.y, q.z, ix, iy, iz);
+            wd = scp->wall_dist0;
+            nearest_wall_part(*scp, c, q.x, q.y, q.z, a.wl, a.skip != 0 ? scp->skip_r : R(INFINITY),
+                              part, wd, wrow, wj);
+        }
+        for (int o = 1; o <= 2; o <<= 1) {
+            const R od = __shfl_xor_sync(0xffffffffu, wd, o);
+            const int orow = __shfl_xor_sync(0xffffffffu, wrow, o);
+            const int oj = __shfl_xor_sync(0xffffffffu, wj, o);
+            if (oj >= 0 && (wj < 0 || od < wd || (od == wd && orow < wrow))) {
+                wd = od;
+                wrow = orow;
+                wj = oj;
+            }
+        }
+        if (part == 0 && sl >= 0 && wj >= 0) {
+            const V4<R> w = ldg4(a.wl.pos + wj), nv = ldg4(a.wl.nrm + wj);
+            if (dot3(q.x - w.x, q.y - w.y, q.z - w.z, nv.x, nv.y, nv.z) >= R(0))
+                a.out.slot[t] = -1 - sl;
+        }
     }
 }
 

@@ -625,7 +625,7 @@ template <class R, class RN> class Solver final : public SolverBase {
 
     // MRRinout over the raw mirrors, one thread per mirror (culled slots turn negative)
     void cull_raw() {
-        k_ph_cull<R, RN><<<std::min(blocks(cap, 256), 148 * 16), 256, 0, stream>>>(args(M1, mcs1));
+        k_ph_cull<R, RN><<<std::min(blocks(4 * cap, 256), 148 * 32), 256, 0, stream>>>(args(M1, mcs1));
         KL();
     }
 

@@ -308,6 +308,75 @@ int mps_adjoint_backward(mps_handle* h, const double* lam_pos, const double* lam
  */
 int mps_get_integrals(mps_handle* h, int32_t scene, double out[6]);
 
+/* ---- the reference's files (host only, no GPU needed) ------------------------------ */
+
+/* MPS_physical.txt: 17 numbers in the order RdDat reads them (kernel.cu:12-22). */
+typedef struct mps_physical {
+    double min[3], max[3];   /* MIN, MAX: domain before the 3.1*l0 padding               */
+    double g[3];             /* G [m/s^2]                                                */
+    double fin_tim;          /* FIN_TIM: end time [s]                                    */
+    double output_time;      /* output_time: interval between output files [s]           */
+    double mach;             /* Mach number: SND = umax / Ma (kernel.cu:408)              */
+    double courant;          /* CRT_NUM (read, unused by the step)                        */
+    double col_rat;          /* COL_RAT                                                  */
+    double dst_lmt_rat;      /* DST_LMT_RAT                                              */
+    double knm_vsc;          /* KNM_VSC                                                  */
+    double pcl_dst;          /* PCL_DST                                                  */
+} mps_physical;
+
+/* Read / write MPS_physical.txt. Every number is read as a float, as RdDat does. */
+int mps_read_physical(const char* path, mps_physical* out);
+int mps_write_physical(const char* path, const mps_physical* ph);
+/*
+ * Read initial.txt (RdDat, kernel.cu:59-131): a count, then one line
+ * 'idx typ x y z nx ny nz g' per particle, read as floats. Particles outside the domain of
+ * `ph` padded by 3.1*l0 are dropped (kernel.cu:121); walls, OBJ and OBJ2 store the negated
+ * file normal, i.e. the inward normal (kernel.cu:126-128), other types a zero normal.
+ * typ[cap], pos and nrm (double SoA) are filled in file order and packed to stride *n_out.
+ * *n_out always receives the number kept; if it exceeds `cap`, or any output pointer is
+ * NULL, MPS_ERR_ARG is returned and nothing else is defined (call again with cap >= *n_out).
+ */
+int mps_read_initial(const char* path, const mps_physical* ph, int32_t cap, int8_t* typ,
+                     double* pos, double* nrm, int32_t* n_out);
+/* Write initial.txt from id-ordered typ/pos/nrm (double SoA, stride n, inward normals). */
+int mps_write_initial(const char* path, int32_t n, const int8_t* typ, const double* pos,
+                      const double* nrm);
+/*
+ * SetPara's derived parameters (kernel.cu:396-415) from the physical file and the scene:
+ * rho = 1000 (const.cuh:37), H = the fluid's extent along the axis of the largest |g|
+ * component (the reference uses y), umax = sqrt(2|g|H), snd = umax / Ma, pmax = rho|g|H,
+ * dt = l0 / (umax + snd). pos is double SoA with stride n.
+ */
+int mps_params_from_physical(const mps_physical* ph, int32_t n, const int8_t* typ,
+                             const double* pos, int32_t precision, mps_params* out);
+
+/* ---- output files (WrtDat / WrtDatWLL / WrtDat2, kernel.cu:161-304) ------------------ */
+
+typedef struct mps_output mps_output;
+/*
+ * Open an output set in directory `dir` (which must exist) for handle `h`, and write the
+ * wall files outputwall00000.csv and outputWLLvec00000.csv of the current state (WrtDatWLL).
+ * The output object keeps device staging and pinned host buffers of the handle's size and
+ * one writer thread. Close it before the handle is destroyed.
+ */
+int mps_output_open(mps_handle* h, const char* dir, mps_output** out);
+/*
+ * WrtDat: write output%05d.csv (fluid: position, velocity, speed, pressure, pav / opt_fqc)
+ * and outputMRR%05d.csv (the second mirror generation, in slot order) for file number
+ * `index`, then set pav = 0 on the device. `opt_fqc` is the number of steps summed into pav
+ * since the last write (the reference's OPT_FQC). The state is copied on the device in the
+ * handle's stream order; the call waits only until the GPU reaches that copy, and the files
+ * are written by the writer thread while the caller queues further steps. One write is in
+ * flight at a time: a second call first waits for the first's files. An I/O error of a
+ * write is reported by the next call on the output object.
+ */
+int mps_output_write(mps_output* o, int32_t index, double opt_fqc);
+/* WrtDat2: write seitei.txt (the fluid as a restart file, kernel.cu:251-276) of the
+ * current state. */
+int mps_output_restart(mps_output* o);
+/* Wait for pending files, release the output object, return the first unreported error. */
+int mps_output_close(mps_output* o);
+
 /* ---- bucket build without allocation ---------------------------------------------- */
 
 #define MPS_NOALLOC_MAX_ITEMS (1 << 20)   /* particles per call                         */

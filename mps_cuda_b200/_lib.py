@@ -64,6 +64,13 @@ class mps_counters(C.Structure):
                 ("reserved", C.c_int32 * 2)]
 
 
+class mps_physical(C.Structure):
+    _fields_ = [("min", C.c_double * 3), ("max", C.c_double * 3), ("g", C.c_double * 3),
+                ("fin_tim", C.c_double), ("output_time", C.c_double), ("mach", C.c_double),
+                ("courant", C.c_double), ("col_rat", C.c_double), ("dst_lmt_rat", C.c_double),
+                ("knm_vsc", C.c_double), ("pcl_dst", C.c_double)]
+
+
 class mps_scene_desc(C.Structure):
     _fields_ = [("l0", C.c_double), ("tank", C.c_double * 3), ("block", C.c_int32 * 3),
                 ("wall_mask", C.c_int32), ("jitter", C.c_double), ("seed", C.c_uint64),
@@ -109,6 +116,17 @@ SIGNATURES = {
     "mps_bucket_build_noalloc": (C.c_int, [C.POINTER(mps_params), C.c_int32, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p]),
+    "mps_read_physical": (C.c_int, [C.c_char_p, C.POINTER(mps_physical)]),
+    "mps_write_physical": (C.c_int, [C.c_char_p, C.POINTER(mps_physical)]),
+    "mps_read_initial": (C.c_int, [C.c_char_p, C.POINTER(mps_physical), C.c_int32, c_int8_p,
+                                   c_double_p, c_double_p, c_int32_p]),
+    "mps_write_initial": (C.c_int, [C.c_char_p, C.c_int32, c_int8_p, c_double_p, c_double_p]),
+    "mps_params_from_physical": (C.c_int, [C.POINTER(mps_physical), C.c_int32, c_int8_p,
+                                           c_double_p, C.c_int32, C.POINTER(mps_params)]),
+    "mps_output_open": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p)]),
+    "mps_output_write": (C.c_int, [C.c_void_p, C.c_int32, C.c_double]),
+    "mps_output_restart": (C.c_int, [C.c_void_p]),
+    "mps_output_close": (C.c_int, [C.c_void_p]),
     "mps_status_string": (C.c_char_p, [C.c_int32]),
     "mps_last_error": (C.c_char_p, []),
 }

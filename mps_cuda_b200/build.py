@@ -21,8 +21,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmps_b200.so")
 SOURCES = ["mps_api.cu", "mps_inst_f32.cu", "mps_inst_f64.cu", "mps_inst_mix.cu",
-           "mps_noalloc.cu", "mps_scene.cpp"]
-HEADERS = ["mps_types.h", "mps_device.cuh", "mps_kernels.cuh", "mps_solver.cuh"]
+           "mps_noalloc.cu", "mps_scene.cpp", "mps_io.cpp", "mps_output.cu"]
+HEADERS = ["mps_types.h", "mps_device.cuh", "mps_kernels.cuh", "mps_adjoint.cuh", "mps_solver.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -79,7 +79,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         objs.append(obj)
     if errors:
         raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
-    cmd = [nvcc, *ARCH, "-shared", "-o", LIB + ".tmp", *objs]
+    cmd = [nvcc, *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lpthread"]
     res = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

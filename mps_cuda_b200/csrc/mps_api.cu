@@ -17,10 +17,6 @@ thread_local std::string g_last_error;
 using mps::ApiError;
 using mps::SolverBase;
 
-struct mps_handle {
-    std::unique_ptr<SolverBase> s;
-};
-
 namespace {
 int fail(int code, const std::string& msg) {
     mps::g_last_error = msg;

@@ -230,10 +230,24 @@ struct SolverBase {
     virtual void get_counters(mps_counters*) = 0;
     virtual void integrals(int scene, double out[6]) = 0;
     virtual void invalidate_graph() = 0;
+    // WrtDat's snapshot into device staging (id order, state type) and the second mirror
+    // generation; the mirror count goes to pinned host memory. Then pav = 0 (kernel.cu:289).
+    virtual void output_snapshot(void* pos, void* vel, void* prs, void* pav, int8_t* typ,
+                                 void* mpos, int* mslot, int* mcount_host) = 0;
+    virtual void get_wall_normals(void* nrm) = 0;  // inward normals, SoA, id order
     virtual void adjoint_record(int nsteps, int every) = 0;
     virtual void adjoint_backward(const double* lam_pos, const double* lam_vel, double* g_pos,
                                   double* g_vel, double* g_nu) = 0;
 };
+
+}  // namespace mps
+
+// the C-ABI's opaque handle: one solver (of one or more scenes)
+struct mps_handle {
+    std::unique_ptr<mps::SolverBase> s;
+};
+
+namespace mps {
 
 template <class R, class RN> class Solver final : public SolverBase {
    public:
@@ -905,6 +919,38 @@ template <class R, class RN> class Solver final : public SolverBase {
         if (pav) CK(cudaMemcpyAsync(io.pav, pav, n1, cudaMemcpyHostToDevice, stream));
         load_fluid(true);
         CK(cudaStreamSynchronize(stream));
+    }
+
+    void output_snapshot(void* pos, void* vel, void* prs, void* pav, int8_t* typ, void* mpos,
+                         int* mslot, int* mcount_host) override {
+        store_all();
+        const size_t n3 = 3 * size_t(nT) * sizeof(R), n1 = size_t(nT) * sizeof(R);
+        CK(cudaMemcpyAsync(pos, io.pos, n3, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(vel, io.vel, n3, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(prs, io.prs, n1, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(pav, io.pav, n1, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(typ, io.typ, nT, cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(mpos, M2.pos, sizeof(V4<R>) * size_t(cap), cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(mslot, M2.slot, sizeof(int) * size_t(cap), cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemcpyAsync(mcount_host, mcs2 + dead(), sizeof(int), cudaMemcpyDeviceToHost, stream));
+        // d_initialize_real_array(d_pav, 0) after WrtDat (kernel.cu:289)
+        CK(cudaMemsetAsync(S.pav, 0, sizeof(R) * size_t(std::max(nF, 1)), stream));
+    }
+
+    void get_wall_normals(void* nrm) override {
+        R* o = static_cast<R*>(nrm);
+        std::memset(o, 0, 3 * size_t(nT) * sizeof(R));
+        if (nW == 0) return;
+        std::vector<V4<R>> n(nW);
+        std::vector<int> ids(nW);
+        CK(cudaMemcpyAsync(n.data(), w_nrm, sizeof(V4<R>) * nW, cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(ids.data(), w_id, sizeof(int) * nW, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        for (int w = 0; w < nW; ++w) {
+            o[ids[w]] = n[w].x;
+            o[size_t(nT) + ids[w]] = n[w].y;
+            o[2 * size_t(nT) + ids[w]] = n[w].z;
+        }
     }
 
     void get_wall_flags(int8_t* out) override {

@@ -129,6 +129,8 @@ class MPSBatch:
     # -- life cycle --------------------------------------------------------------------
     def close(self):
         if getattr(self, "_h", None):
+            for o in list(getattr(self, "_outputs", ())):  # output sets read this handle
+                o.close()
             lib().mps_destroy(self._h)
             self._h = None
 

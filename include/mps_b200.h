@@ -149,9 +149,18 @@ enum {
     MPS_OPT_GRAPH = 1,       /* 1: replay mps_step through a captured CUDA graph        */
     MPS_OPT_BLOCK = 2,       /* threads per block of the neighbour passes (0 = tuned)   */
     MPS_OPT_CELL_SKIP = 3,   /* 1: skip bucket rows outside the radius (default 1)      */
-    MPS_OPT_TIMING = 4       /* 1: time every kernel group of mps_step with CUDA events
+    MPS_OPT_TIMING = 4,      /* 1: time every kernel group of mps_step with CUDA events
                                 on the handle's stream (steps then run without a graph) */
+    MPS_OPT_GRADIENT = 5     /* PrsGrdTrm variant, MPS_GRAD_* (default STANDARD)        */
 };
+
+/* PrsGrdTrm variants (MPS_OPT_GRADIENT). STANDARD is the kernel the reference compiles
+ * (kernel.cu:1651-1794). CORRECTED is its `#if 0` alternative (kernel.cu:1435-1648): the
+ * moment matrix M = sum w r r^T / n0_grad of the fluid and mirror neighbours inside rp is
+ * inverted and a = -1/rho M^-1 sum w (P_j - P_min) r / n0_grad. As in the reference, a
+ * particle whose M is all zero keeps ChkCol's velocity as its acceleration, and a singular M
+ * gives non-finite values, which ChkPcl deletes. The adjoint supports STANDARD only. */
+enum { MPS_GRAD_STANDARD = 0, MPS_GRAD_CORRECTED = 1 };
 
 /* Kernel groups reported by mps_get_timing. */
 enum {

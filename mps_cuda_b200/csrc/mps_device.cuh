@@ -430,14 +430,79 @@ __device__ __forceinline__ R eos(const SceneDev<R, RN>& sc, RN ni) {
 }
 
 // ---- PrsGrdTrm (kernel.cu:1678-1791) ----------------------------------------------------
+// The sums over the neighbours inside rp, w = WEI_grad(d, rp) / d^2 and r = x_j - x_i.
+// GradPlain is the compiled variant: b = sum w (P_j - P_min) r (kernel.cu:1728-1735).
+// GradCorr is the corrected-matrix #if 0 variant (kernel.cu:1535-1548): also the moment
+// matrix M = sum w r r^T, entry (a, b) accumulated as (w r_a) r_b, all nine kept apart.
+template <class R> struct GradPlain {
+    R sx = R(0), sy = R(0), sz = R(0);
+    __device__ __forceinline__ void add(R w, R pd, R dx, R dy, R dz) {
+        const R pw = pd * w;
+        sx = fmaR(pw, dx, sx);
+        sy = fmaR(pw, dy, sy);
+        sz = fmaR(pw, dz, sz);
+    }
+};
+template <class R> struct GradCorr {
+    R m0 = R(0), m1 = R(0), m2 = R(0), m3 = R(0), m4 = R(0), m5 = R(0), m6 = R(0), m7 = R(0),
+      m8 = R(0);
+    R b0 = R(0), b1 = R(0), b2 = R(0);
+    __device__ __forceinline__ void add(R w, R pd, R dx, R dy, R dz) {
+        const R wx = w * dx, wy = w * dy, wz = w * dz;
+        m0 = fmaR(wx, dx, m0); m1 = fmaR(wx, dy, m1); m2 = fmaR(wx, dz, m2);
+        m3 = fmaR(wy, dx, m3); m4 = fmaR(wy, dy, m4); m5 = fmaR(wy, dz, m5);
+        m6 = fmaR(wz, dx, m6); m7 = fmaR(wz, dy, m7); m8 = fmaR(wz, dz, m8);
+        const R wp = w * pd;
+        b0 = fmaR(wp, dx, b0);
+        b1 = fmaR(wp, dy, b1);
+        b2 = fmaR(wp, dz, b2);
+    }
+};
+
+// acceleration of the compiled variant: -1/rho * b * 3/n0_grad (kernel.cu:1788-1790)
+template <class R, class RN>
+__device__ __forceinline__ bool grad_acc(const SceneDev<R, RN>& sc, const GradPlain<R>& g, R& ax,
+                                         R& ay, R& az) {
+    ax = (sc.invro * g.sx) * sc.a3;
+    ay = (sc.invro * g.sy) * sc.a3;
+    az = (sc.invro * g.sz) * sc.a3;
+    return true;
+}
+// of the corrected variant: M and b scaled by 1/n0_grad, M inverted through its adjugate and
+// determinant, a = -1/rho M^-1 b (kernel.cu:1608-1642). False when all nine entries of M are
+// zero: the reference then returns without writing d_Acc (kernel.cu:1620).
+template <class R, class RN>
+__device__ __forceinline__ bool grad_acc(const SceneDev<R, RN>& sc, const GradCorr<R>& g, R& ax,
+                                         R& ay, R& az) {
+    const R k = sc.invn0g;
+    const R m0 = k * g.m0, m1 = k * g.m1, m2 = k * g.m2, m3 = k * g.m3, m4 = k * g.m4,
+            m5 = k * g.m5, m6 = k * g.m6, m7 = k * g.m7, m8 = k * g.m8;
+    if (m0 == R(0) && m1 == R(0) && m2 == R(0) && m3 == R(0) && m4 == R(0) && m5 == R(0) &&
+        m6 == R(0) && m7 == R(0) && m8 == R(0))
+        return false;
+    const R det = R(1) / ((m0 * m4 * m8 + m1 * m5 * m6 + m2 * m3 * m7) -
+                          (m2 * m4 * m6 + m0 * m5 * m7 + m1 * m3 * m8));
+    const R l0 = det * (m4 * m8 - m5 * m7), l1 = det * -(m1 * m8 - m2 * m7),
+            l2 = det * (m1 * m5 - m2 * m4);
+    const R l3 = det * -(m3 * m8 - m5 * m6), l4 = det * (m0 * m8 - m2 * m6),
+            l5 = det * -(m0 * m5 - m2 * m3);
+    const R l6 = det * (m3 * m7 - m4 * m6), l7 = det * -(m0 * m7 - m1 * m6),
+            l8 = det * (m0 * m4 - m1 * m3);
+    const R r0 = k * g.b0, r1 = k * g.b1, r2 = k * g.b2;
+    ax = sc.invro * (l0 * r0 + l1 * r1 + l2 * r2);
+    ay = sc.invro * (l3 * r0 + l4 * r1 + l5 * r2);
+    az = sc.invro * (l6 * r0 + l7 * r1 + l8 * r2);
+    return true;
+}
+
 // mirror part; the reference skips the mirror whose slot index equals i (kernel.cu:1759).
 // Slots are stored as global_owner_id * NumMRR + k: the local slot is that minus
 // NumMRR * pbase, the local particle index is pid_local.
-template <class R, class RN>
+template <class R, class RN, class G>
 __device__ __forceinline__ void grad_sum_mirrors(const SceneDev<R, RN>& sc, const RowCtx<R>& c,
                                                  int pid_local, R x, R y, R z, R pmin,
-                                                 const MirrorView<R>& m, bool skip, R& sx, R& sy,
-                                                 R& sz, int& cm) {
+                                                 const MirrorView<R>& m, bool skip, G& g,
+                                                 int& cm) {
     const R B = skip ? sc.skip_rp : R(INFINITY);
     const int skip_slot = pid_local + kNumMRR * sc.pbase;
     for_rows(sc, m.cs, c, B, [&](int k) {
@@ -447,23 +512,19 @@ __device__ __forceinline__ void grad_sum_mirrors(const SceneDev<R, RN>& sc, cons
         R d2 = dot3(dx, dy, dz, dx, dy, dz);
         if (d2 < sc.rp2) {
             R d = sqrtR(d2);
-            R w = wei_grad(d, sc.rp) / d2;
-            R pw = (q.w - pmin) * w;
-            sx = fmaR(pw, dx, sx);
-            sy = fmaR(pw, dy, sy);
-            sz = fmaR(pw, dz, sz);
+            g.add(wei_grad(d, sc.rp) / d2, q.w - pmin, dx, dy, dz);
             ++cm;
         }
     });
 }
 
-template <class R, class RN>
+template <class R, class RN, class G>
 __device__ __forceinline__ void grad_sum(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
                                          int pid_local, R x, R y, R z, R pi,
                                          const int* __restrict__ csr,
                                          const V4<R>* __restrict__ posf,
                                          const R* __restrict__ prs, const MirrorView<R>& m,
-                                         bool skip, R& sx, R& sy, R& sz, int& cf, int& cm) {
+                                         bool skip, G& g, int& cf, int& cm) {
     R B = skip ? sc.skip_rp : R(INFINITY);
     R pmin = pi;
     for_fluid(sc, csr, posf, c, B, [&](int j, const V4<R>& q) {
@@ -481,26 +542,22 @@ __device__ __forceinline__ void grad_sum(const SceneDev<R, RN>& sc, const RowCtx
         R d2 = dot3(dx, dy, dz, dx, dy, dz);
         if (d2 < sc.rp2) {
             R d = sqrtR(d2);
-            R w = wei_grad(d, sc.rp) / d2;
-            R pw = (__ldg(prs + j) - pmin) * w;
-            sx = fmaR(pw, dx, sx);
-            sy = fmaR(pw, dy, sy);
-            sz = fmaR(pw, dz, sz);
+            g.add(wei_grad(d, sc.rp) / d2, __ldg(prs + j) - pmin, dx, dy, dz);
             ++cf;
         }
     });
-    grad_sum_mirrors(sc, c, pid_local, x, y, z, pmin, m, skip, sx, sy, sz, cm);
+    grad_sum_mirrors(sc, c, pid_local, x, y, z, pmin, m, skip, g, cm);
 }
 
 // out-of-line copy for the rare slot whose neighbour list overflowed its capacity
-template <class R, class RN>
+template <class R, class RN, class G>
 __device__ __noinline__ void grad_sum_outline(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
                                               int pid_local, R x, R y, R z, R pi,
                                               const int* __restrict__ csr,
                                               const V4<R>* __restrict__ posf,
                                               const R* __restrict__ prs, const MirrorView<R>& m,
-                                              bool skip, R& sx, R& sy, R& sz, int& cf, int& cm) {
-    grad_sum(sc, c, s, pid_local, x, y, z, pi, csr, posf, prs, m, skip, sx, sy, sz, cf, cm);
+                                              bool skip, G& g, int& cf, int& cm) {
+    grad_sum(sc, c, s, pid_local, x, y, z, pi, csr, posf, prs, m, skip, g, cf, cm);
 }
 
 // ---- GenMRR_nonslip for one fluid particle (kernel.cu:726-891) ---------------------------

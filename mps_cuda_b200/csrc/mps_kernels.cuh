@@ -14,6 +14,8 @@
 // Mirrors produced by pass C are the next step's first generation: GenMRR at the start of
 // the next step (kernel.cu:1906-1908) would read the same positions and pressures.
 #pragma once
+#include <type_traits>
+
 #include "mps_device.cuh"
 
 namespace mps {
@@ -106,31 +108,41 @@ __global__ void k_bin_key(Src src, const int* n_ptr, int n_fixed, int* __restric
     }
 }
 
-// k_bin_key for the fluid: also counts each fine cell's items at its row-major index
+constexpr int kScan16Threads = 512, kScan16Per = 16, kScan16Tile = kScan16Threads * kScan16Per;
+
+// k_bin_key for the fluid: counts each fine cell's items at its bucket-major index (count)
+// and at its row-major index (count_r), and adds every item to the total of its scan tile
+// (kScan16Tile cells) in both orders (part, part_r), so that k_fine_scan needs no reduce pass.
+// The tile totals take one atomic per tile a warp touches.
 template <class R, class RN>
 __global__ void k_bin_key_fluid(FluidKeySrc<R, RN> src, int n, int* __restrict__ key,
                                 int* __restrict__ rnk, int* __restrict__ count,
-                                int* __restrict__ count_r, DevCounters* cnt) {
+                                int* __restrict__ count_r, int* __restrict__ part,
+                                int* __restrict__ part_r, DevCounters* cnt) {
     const int lane = threadIdx.x & 31;
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
-        int t = base + lane;
-        bool act = t < n;
-        int c = act ? src.key(t, cnt) : -1;
-        unsigned peers = __match_any_sync(0xffffffffu, c);
-        int leader = __ffs(peers) - 1;
-        int below = __popc(peers & ((1u << lane) - 1));
+        const int t = base + lane;
+        const bool act = t < n;
+        const int c = act ? src.key(t, cnt) : -1;
+        int cr = c;
+        if (act && c != src.dead) {
+            const SceneDev<R, RN>& s =
+                src.sc[src.nscene > 1 ? scene_of(src.sc, src.nscene, src.pid[t]) : 0];
+            cr = fine_rowmajor(s, c);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, c);
+        const int leader = __ffs(peers) - 1;
+        const int below = __popc(peers & ((1u << lane) - 1));
         int b = 0;
         if (act && lane == leader) {
             b = atomicAdd(&count[c], __popc(peers));
-            int cr = c;
-            if (c != src.dead) {
-                const SceneDev<R, RN>& s =
-                    src.sc[src.nscene > 1 ? scene_of(src.sc, src.nscene, src.pid[t]) : 0];
-                cr = fine_rowmajor(s, c);
-            }
             atomicAdd(&count_r[cr], __popc(peers));
         }
+        const unsigned tf = __match_any_sync(0xffffffffu, act ? c / kScan16Tile : -1);
+        const unsigned tr = __match_any_sync(0xffffffffu, act ? cr / kScan16Tile : -1);
+        if (act && lane == __ffs(tf) - 1) atomicAdd(&part[c / kScan16Tile], __popc(tf));
+        if (act && lane == __ffs(tr) - 1) atomicAdd(&part_r[cr / kScan16Tile], __popc(tr));
         b = __shfl_sync(0xffffffffu, b, leader);
         if (act) {
             key[t] = c;
@@ -326,10 +338,9 @@ static __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int* _
     if (base <= L - 1 && L - 1 < base + kScanPer) out[L] = excl;  // thread holding the last item
 }
 
-// Scan of the fluid's fine-cell counts: 16 counts per thread through int4 loads, and the
-// counts cleared as they are read, so that the next bucket build starts from zeros without
-// a memset (the fine tables are 27 times the bucket count).
-constexpr int kScan16Threads = 512, kScan16Per = 16, kScan16Tile = kScan16Threads * kScan16Per;
+// Scan of the fluid's fine-cell counts (fine_scan below): 16 counts per thread through int4
+// loads, and the counts cleared as they are read, so that the next bucket build starts from
+// zeros without a memset (the fine tables are 27 times the bucket count).
 
 __device__ __forceinline__ void load16(const int* __restrict__ in, int base, int L, int v[16]) {
     if (base + 16 <= L) {
@@ -345,24 +356,27 @@ __device__ __forceinline__ void load16(const int* __restrict__ in, int base, int
     }
 }
 
-static __global__ void __launch_bounds__(kScan16Threads) k_scan16_reduce(const int* __restrict__ in,
-                                                                     int L, int* __restrict__ part) {
-    __shared__ int sh[32];
-    int v[16];
-    load16(in, blockIdx.x * kScan16Tile + threadIdx.x * kScan16Per, L, v);
-    int s = 0;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) s += v[k];
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = s;
-}
+// The two fine-cell tables of a fluid bucket build: count[k] (k = 0: bucket-major, 1:
+// row-major) with its per-tile totals part[k] from k_bin_key_fluid, scanned into out[k].
+struct FineScan {
+    int* count[2];
+    int* part[2];
+    int* out[2];
+    int L, ntile;
+    int* ticket;  // blocks finished; zero between launches
+};
 
-// exclusive scan of in[0..L) into out[0..L], out[L] = total; in[0..L) is left zero
-static __global__ void __launch_bounds__(kScan16Threads) k_scan16_apply(int* __restrict__ in, int L,
-                                                                    const int* __restrict__ part,
-                                                                    int* __restrict__ out) {
+// Exclusive scan of count[k][0..L) into out[k][0..L], out[k][L] = total, for k = blockIdx.y.
+// The counts are left zero; the last block to finish also zeroes the tile totals for the
+// next build (every block has read them by then).
+static __global__ void __launch_bounds__(kScan16Threads) k_fine_scan(FineScan f) {
     __shared__ int sh[32];
     __shared__ int wsum[32];
+    __shared__ int last;
+    const int which = blockIdx.y, L = f.L;
+    int* __restrict__ in = f.count[which];
+    const int* __restrict__ part = f.part[which];
+    int* __restrict__ out = f.out[which];
     int off = 0;
     for (int b = threadIdx.x; b < (int)blockIdx.x; b += blockDim.x) off += part[b];
     off = block_sum(off, sh);
@@ -413,6 +427,19 @@ static __global__ void __launch_bounds__(kScan16Threads) k_scan16_apply(int* __r
             }
     }
     if (base <= L - 1 && L - 1 < base + kScan16Per) out[L] = excl;  // thread holding the last item
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(f.ticket, 1) == int(gridDim.x * gridDim.y) - 1;
+    }
+    __syncthreads();
+    if (last) {
+        for (int k = threadIdx.x; k < f.ntile; k += blockDim.x) {
+            f.part[0][k] = 0;
+            f.part[1][k] = 0;
+        }
+        if (threadIdx.x == 0) *f.ticket = 0;
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -703,9 +730,13 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
 }
 
 // pass C: PrsGrdTrm (kernel.cu:1651-1794) + UpPcl2/ChkPcl (kernel.cu:1815-1829), walking
-// the neighbour lists pass B left. TAPE: also keeps the velocity before the clamp.
-template <class R, class RN, bool DIAG, bool TAPE = false>
-__global__ void __launch_bounds__(128, 10) k_pass_c(PassArgs<R, RN> a) {
+// the neighbour lists pass B left. TAPE: also keeps the velocity before the clamp. CORR: the
+// corrected-matrix PrsGrdTrm (kernel.cu:1435-1648); where its moment matrix is all zero the
+// reference leaves in d_Acc the velocity ChkCol stored there (kernel.cu:1275, 1620), which
+// UpPcl2 then applies as the acceleration: the velocity after pass B, as here.
+template <class R, class RN, bool DIAG, bool TAPE = false, bool CORR = false>
+__global__ void __launch_bounds__(128, CORR ? 6 : 10) k_pass_c(PassArgs<R, RN> a) {
+    using G = typename std::conditional<CORR, GradCorr<R>, GradPlain<R>>::type;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
     const int nalive = __ldg(a.cs + a.dead);
@@ -722,7 +753,7 @@ __global__ void __launch_bounds__(128, 10) k_pass_c(PassArgs<R, RN> a) {
     int ix, iy, iz;
     cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
     RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
-    R sx = 0, sy = 0, sz = 0;
+    G g;
     int cf = 0, cm = 0;
     const int n = a.nbcnt[s];
     if (n <= a.nbK) {
@@ -759,11 +790,7 @@ __global__ void __launch_bounds__(128, 10) k_pass_c(PassArgs<R, RN> a) {
             R d2 = dot3(dx, dy, dz, dx, dy, dz);
             if (d2 < rp2) {
                 R d = sqrtR(d2);
-                R w = wei_grad(d, rp) / d2;
-                R pw = (__ldg(prs + j) - pmin) * w;
-                sx = fmaR(pw, dx, sx);
-                sy = fmaR(pw, dy, sy);
-                sz = fmaR(pw, dz, sz);
+                g.add(wei_grad(d, rp) / d2, __ldg(prs + j) - pmin, dx, dy, dz);
                 ++cf;
             }
         };
@@ -780,14 +807,18 @@ __global__ void __launch_bounds__(128, 10) k_pass_c(PassArgs<R, RN> a) {
             const int j = nb[k * st];
             gr(j, ldg4(pos + j));
         }
-        grad_sum_mirrors(sc, c, pid - sc.pbase, p.x, p.y, p.z, pmin, a.m, a.skip != 0, sx, sy, sz,
-                         cm);
+        grad_sum_mirrors(sc, c, pid - sc.pbase, p.x, p.y, p.z, pmin, a.m, a.skip != 0, g, cm);
     } else {
         grad_sum_outline(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, pi, a.csr, a.posf, a.tprs, a.m,
-                         a.skip != 0, sx, sy, sz, cf, cm);
+                         a.skip != 0, g, cf, cm);
     }
-    R ax = (sc.invro * sx) * sc.a3, ay = (sc.invro * sy) * sc.a3, az = (sc.invro * sz) * sc.a3;
     V4<R> v = a.tvel[s];
+    R ax, ay, az;
+    if (!grad_acc(sc, g, ax, ay, az)) {
+        ax = v.x;
+        ay = v.y;
+        az = v.z;
+    }
     R ux = fmaR(ax, sc.dt, v.x), uy = fmaR(ay, sc.dt, v.y), uz = fmaR(az, sc.dt, v.z);
     R x = fmaR(ax * sc.dt, sc.dt, p.x), y = fmaR(ay * sc.dt, sc.dt, p.y),
       z = fmaR(az * sc.dt, sc.dt, p.z);
@@ -966,8 +997,9 @@ __global__ void __launch_bounds__(128) k_ph_prs(PassArgs<R, RN> a) {
     }
 }
 
-template <class R, class RN, bool DIAG>
+template <class R, class RN, bool DIAG, bool CORR = false>
 __global__ void __launch_bounds__(128) k_ph_grd(PassArgs<R, RN> a) {
+    using G = typename std::conditional<CORR, GradCorr<R>, GradPlain<R>>::type;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF || a.typ[s] != kFLD) return;
     const int pid = a.pid[s];
@@ -976,12 +1008,12 @@ __global__ void __launch_bounds__(128) k_ph_grd(PassArgs<R, RN> a) {
     int ix, iy, iz;
     cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
     RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
-    R sx = 0, sy = 0, sz = 0;
+    G g;
     int cf = 0, cm = 0;
     grad_sum(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, a.prs[s], a.csr, a.posf, a.prs, a.m,
-             a.skip != 0, sx, sy, sz, cf, cm);
-    a.acc[s] = V4<R>{(sc.invro * sx) * sc.a3, (sc.invro * sy) * sc.a3, (sc.invro * sz) * sc.a3,
-                     R(0)};
+             a.skip != 0, g, cf, cm);
+    R ax, ay, az;
+    if (grad_acc(sc, g, ax, ay, az)) a.acc[s] = V4<R>{ax, ay, az, R(0)};  // else d_Acc stays
     if (DIAG) {
         int32_t* d = a.diag + size_t(pid) * kDiagCols;
         d[DG_GRD_F] = cf;

@@ -135,6 +135,7 @@ static void derive_scene(const mps_params& p, int cbase, int fbase, int pbase, i
     s.colfac = (col * rho) / (rho + rho);
     s.invro = R(-1) / rho;
     s.a3 = R(3) / n0_grad;
+    s.invn0g = R(1) / n0_grad;
     const double m = 1e-3 * double(db);
     auto sq = [&](double v) { return R((v + m) * (v + m)); };
     s.skip_r = sq(double(r));
@@ -210,6 +211,7 @@ struct SolverBase {
     std::vector<int> counts;
     bool diag_on = false, graph_on = false;
     int skip_opt = 1, block = 128;
+    int grad_mode = MPS_GRAD_STANDARD;  // PrsGrdTrm variant (MPS_OPT_GRADIENT)
     long long steps = 0;
     long long launches = 0;       // kernels launched (graph replays included)
     long long body_launches = 0;  // kernels of one captured step
@@ -268,6 +270,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     // fluid positions in row-major fine-cell order (slot in w) and that order's cell starts
     V4<R>* posf;
     int *csr, *count_f, *count_r;
+    int *part_f, *part_r;  // per scan tile totals of count_f / count_r (k_bin_key_fluid)
     bool posf_stale = false;  // particles moved in place since the copy was made
     // bucket-build scratch
     int *key, *rnk, *seg, *count, *part;
@@ -501,6 +504,11 @@ template <class R, class RN> class Solver final : public SolverBase {
         count_r = ar.template get<int>(size_t(LF()));
         CK(cudaMemsetAsync(count_f, 0, sizeof(int) * size_t(LF()), stream));
         CK(cudaMemsetAsync(count_r, 0, sizeof(int) * size_t(LF()), stream));
+        const size_t ntile = (size_t(LF()) + kScan16Tile - 1) / kScan16Tile;
+        part_f = ar.template get<int>(ntile);
+        part_r = ar.template get<int>(ntile);
+        CK(cudaMemsetAsync(part_f, 0, sizeof(int) * ntile, stream));
+        CK(cudaMemsetAsync(part_r, 0, sizeof(int) * ntile, stream));
         posf = ar.template get<V4<R>>(F);
         for (MirrorBuf<R>* b : {&U, &M1, &M2}) {
             b->pos = ar.template get<V4<R>>(cap);
@@ -513,8 +521,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         rnk = ar.template get<int>(items);
         seg = ar.template get<int>(items);
         count = ar.template get<int>(L());
-        part = ar.template get<int>((size_t(LF()) + kScan16Tile - 1) / kScan16Tile +
-                                    (L() + kScanTile - 1) / kScanTile + 1);
+        part = ar.template get<int>((L() + kScanTile - 1) / kScanTile + 1);
         d_fluid_ids = ar.template get<int>(F);
         d_wall_ids = ar.template get<int>(W);
         d_nF = ar.template get<int>(1);
@@ -578,17 +585,13 @@ template <class R, class RN> class Solver final : public SolverBase {
         const int ncell = LF();
         const int grid = std::min(blocks(std::max(nF, 1), 256), 148 * 32);
         if (nF > 0) {
-            k_bin_key_fluid<R, RN><<<grid, 256, 0, stream>>>(ks, nF, key, rnk, count_f, count_r, cnt);
+            k_bin_key_fluid<R, RN><<<grid, 256, 0, stream>>>(ks, nF, key, rnk, count_f, count_r,
+                                                             part_f, part_r, cnt);
             KL();
         }
         const int nb = (ncell + kScan16Tile - 1) / kScan16Tile;
-        k_scan16_reduce<<<nb, kScan16Threads, 0, stream>>>(count_f, ncell, part);
-        KL();
-        k_scan16_apply<<<nb, kScan16Threads, 0, stream>>>(count_f, ncell, part, cs);
-        KL();
-        k_scan16_reduce<<<nb, kScan16Threads, 0, stream>>>(count_r, ncell, part);
-        KL();
-        k_scan16_apply<<<nb, kScan16Threads, 0, stream>>>(count_r, ncell, part, csr);
+        FineScan fs{{count_f, count_r}, {part_f, part_r}, {cs, csr}, ncell, nb, &cnt->scan_ticket};
+        k_fine_scan<<<dim3(nb, 2), kScan16Threads, 0, stream>>>(fs);
         KL();
         if (nF > 0) {
             k_bin_seg<FluidKeySrc<R, RN>><<<grid, 256, 0, stream>>>(ks, nullptr, nF, key, rnk, cs, seg);
@@ -674,7 +677,10 @@ template <class R, class RN> class Solver final : public SolverBase {
         // pass C: PrsGrdTrm + UpPcl2, then the first mirror generation of the next step
         {
             Scope t(this, MPS_K_PASS_C);
-            k_pass_c<R, RN, D><<<blocks(nF, bc), bc, 0, stream>>>(args(M2, mcs2));
+            if (grad_mode == MPS_GRAD_CORRECTED)
+                k_pass_c<R, RN, D, false, true><<<blocks(nF, bc), bc, 0, stream>>>(args(M2, mcs2));
+            else
+                k_pass_c<R, RN, D><<<blocks(nF, bc), bc, 0, stream>>>(args(M2, mcs2));
             KL();
         }
         reset_raw();
@@ -856,8 +862,13 @@ template <class R, class RN> class Solver final : public SolverBase {
                 break;
             case MPS_PHASE_PRSGRDTRM:
                 need_lists();
-                if (diag_on) k_ph_grd<R, RN, true><<<gb, block, 0, stream>>>(a);
-                else k_ph_grd<R, RN, false><<<gb, block, 0, stream>>>(a);
+                if (grad_mode == MPS_GRAD_CORRECTED) {
+                    if (diag_on) k_ph_grd<R, RN, true, true><<<gb, block, 0, stream>>>(a);
+                    else k_ph_grd<R, RN, false, true><<<gb, block, 0, stream>>>(a);
+                } else {
+                    if (diag_on) k_ph_grd<R, RN, true><<<gb, block, 0, stream>>>(a);
+                    else k_ph_grd<R, RN, false><<<gb, block, 0, stream>>>(a);
+                }
                 KL();
                 acc_dirty = true;
                 break;
@@ -1130,6 +1141,9 @@ template <class R, class RN> class Solver final : public SolverBase {
     }
 
     void adjoint_record(int nsteps, int every) override {
+        if (grad_mode != MPS_GRAD_STANDARD)
+            throw ApiError(MPS_ERR_UNSUPPORTED,
+                           "the adjoint covers the default PrsGrdTrm only (MPS_GRAD_STANDARD)");
         if (nscene != 1)
             throw ApiError(MPS_ERR_UNSUPPORTED, "the adjoint runs on single-scene handles");
         if (nsteps <= 0 || every <= 0)

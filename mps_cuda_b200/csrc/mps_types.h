@@ -51,6 +51,7 @@ template <class R, class RN> struct SceneDev {
     R lo[3], hi[3];   // ChkPcl box (kernel.cu:484-486)
     R colfac;         // COL * mj / (mi + mj) (kernel.cu:1215)
     R invro, a3;      // -1/rho, 3/n0_grad (kernel.cu:1659, 1665)
+    R invn0g;         // 1/n0_grad (kernel.cu:1443, the corrected-gradient variant)
     // (radius + margin)^2 used to skip bucket rows: r, rp, rlim, 0.45 l0, max(rlim, rp)
     R skip_r, skip_rp, skip_rl, skip_rw, skip_rc;
     RN n0g, prs_coef, pmax, rho;          // number density / EOS in RN (kernel.cu:1388-1406)
@@ -65,7 +66,8 @@ struct DevCounters {
     int err_nan;          // non-finite position met in a bucket build
     int n_m1, n_m2;       // alive mirrors after the latest generations
     int deleted;          // particles deleted by ChkPcl (cumulative)
-    int pad[8];
+    int scan_ticket;      // blocks of the running fine-cell scan that finished (0 between)
+    int pad[7];
 };
 
 }  // namespace mps

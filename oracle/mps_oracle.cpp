@@ -80,6 +80,7 @@ struct Oracle {
     int numn0_grad;
     RN n0_grad_n, prs_coef_n, pmax_n, rho_n;
     R rlim2, col, rho, knm, snd, prs_coef, pmax, umax, dt, rlim_wall2, edge_r2;
+    int grad_mode = 0;  // 0: PrsGrdTrm as compiled (kernel.cu:1651-1794), 1: the #if 0 variant
 
     int n;
     std::vector<int8_t> typ, wse;
@@ -641,8 +642,93 @@ struct Oracle {
         }
     }
 
+    // ---- PrsGrdTrm, corrected-matrix variant (the #if 0 branch, kernel.cu:1435-1648) -------
+    // P_min as in the active variant; then the moment matrix sum w r r^T (nine sums, each
+    // row a times column b as (w r_a) r_b) and the right side sum w (P_j - P_min) r over the
+    // fluid and mirror neighbours inside rp, both scaled by 1/n0_grad; the acceleration is
+    // -1/rho M^-1 b through the adjugate over the determinant (kernel.cu:1622-1642). When all
+    // nine sums are zero the reference returns without writing d_Acc (kernel.cu:1620), which
+    // then still holds the velocity ChkCol stored there (kernel.cu:1275): that is kept.
+    void prsgrdtrm_corrected() {
+        const R invro = R(-1) / rho;
+        const R invn0 = R(1) / n0_grad;
+#pragma omp parallel for schedule(dynamic, 256)
+        for (int i = 0; i < n; ++i) {
+            if (typ[i] != FLD) continue;
+            R x = px[i], y = py[i], z = pz[i];
+            R pmin = prs[i];
+            int ix, iy, iz;
+            cell3(x, y, z, ix, iy, iz);
+            for_fluid(x, y, z, ix, iy, iz, rp, [&](int j) {
+                if (j == i || typ[j] != FLD) return;
+                R qx = px[j] - x, qy = py[j] - y, qz = pz[j] - z;
+                R d2 = dot3(qx, qy, qz, qx, qy, qz);
+                if (d2 < rp2) {
+                    if (prs[j] < pmin) pmin = prs[j];
+                }
+            });
+            R m[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, b[3] = {0, 0, 0};
+            int cf = 0, cm = 0;
+            auto add = [&](R qx, R qy, R qz, R d2, R pj) {
+                R d = std::sqrt(d2);
+                R w = wei_grad(d, rp) / d2;
+                R wx = w * qx, wy = w * qy, wz = w * qz;
+                m[0] = fmar(wx, qx, m[0]); m[1] = fmar(wx, qy, m[1]); m[2] = fmar(wx, qz, m[2]);
+                m[3] = fmar(wy, qx, m[3]); m[4] = fmar(wy, qy, m[4]); m[5] = fmar(wy, qz, m[5]);
+                m[6] = fmar(wz, qx, m[6]); m[7] = fmar(wz, qy, m[7]); m[8] = fmar(wz, qz, m[8]);
+                R wp = w * (pj - pmin);
+                b[0] = fmar(wp, qx, b[0]); b[1] = fmar(wp, qy, b[1]); b[2] = fmar(wp, qz, b[2]);
+            };
+            for_fluid(x, y, z, ix, iy, iz, rp, [&](int j) {
+                if (j == i || typ[j] != FLD) return;
+                R qx = px[j] - x, qy = py[j] - y, qz = pz[j] - z;
+                R d2 = dot3(qx, qy, qz, qx, qy, qz);
+                if (d2 < rp2) {
+                    add(qx, qy, qz, d2, prs[j]);
+                    ++cf;
+                }
+            });
+            for_nb(mstart, mlist, ix, iy, iz, [&](int s) {
+                if (s == i) return;  // the slot-index quirk of the active variant (:1575)
+                R qx = mx[s] - x, qy = my[s] - y, qz = mz[s] - z;
+                R d2 = dot3(qx, qy, qz, qx, qy, qz);
+                if (d2 < rp2) {
+                    add(qx, qy, qz, d2, mprs[s]);
+                    ++cm;
+                }
+            });
+            diag[size_t(i) * D_NCOL + D_GRD_F] = cf;
+            diag[size_t(i) * D_NCOL + D_GRD_M] = cm;
+            bool zero = true;
+            for (int k = 0; k < 9; ++k) {
+                m[k] = invn0 * m[k];
+                zero = zero && m[k] == R(0);
+            }
+            if (zero) continue;  // d_Acc keeps ChkCol's velocity
+            const R det = R(1) / ((m[0] * m[4] * m[8] + m[1] * m[5] * m[6] + m[2] * m[3] * m[7]) -
+                                  (m[2] * m[4] * m[6] + m[0] * m[5] * m[7] + m[1] * m[3] * m[8]));
+            const R l0_ = det * (m[4] * m[8] - m[5] * m[7]);
+            const R l1_ = det * -(m[1] * m[8] - m[2] * m[7]);
+            const R l2_ = det * (m[1] * m[5] - m[2] * m[4]);
+            const R l3_ = det * -(m[3] * m[8] - m[5] * m[6]);
+            const R l4_ = det * (m[0] * m[8] - m[2] * m[6]);
+            const R l5_ = det * -(m[0] * m[5] - m[2] * m[3]);
+            const R l6_ = det * (m[3] * m[7] - m[4] * m[6]);
+            const R l7_ = det * -(m[0] * m[7] - m[1] * m[6]);
+            const R l8_ = det * (m[0] * m[4] - m[1] * m[3]);
+            const R r0 = invn0 * b[0], r1 = invn0 * b[1], r2_ = invn0 * b[2];
+            ax[i] = invro * (l0_ * r0 + l1_ * r1 + l2_ * r2_);
+            ay[i] = invro * (l3_ * r0 + l4_ * r1 + l5_ * r2_);
+            az[i] = invro * (l6_ * r0 + l7_ * r1 + l8_ * r2_);
+        }
+    }
+
     // ---- PrsGrdTrm, active variant (kernel.cu:1651-1794) ----------------------------------
     void prsgrdtrm() {
+        if (grad_mode == 1) {
+            prsgrdtrm_corrected();
+            return;
+        }
         const R invro = R(-1) / rho;
         const R a3 = R(3) / n0_grad;
 #pragma omp parallel for schedule(dynamic, 256)
@@ -822,6 +908,14 @@ int oracle_set_threads(int32_t n) {
 
 int oracle_phase(void* h, int32_t ph) {
     return dispatch(h, [&](auto& o) { return o.phase(ph); });
+}
+
+int oracle_set_gradient(void* h, int32_t mode) {
+    if (mode < 0 || mode > 1) return 1;
+    return dispatch(h, [&](auto& o) {
+        o.grad_mode = mode;
+        return 0;
+    });
 }
 
 int oracle_step(void* h, int32_t k) {

@@ -32,6 +32,9 @@ int oracle_set_threads(int32_t n);
 /* phase numbering is MPS_PHASE_* of include/mps_b200.h */
 int oracle_phase(void* h, int32_t phase);
 int oracle_step(void* h, int32_t nsteps);
+/* PrsGrdTrm variant: 0 as compiled (kernel.cu:1651-1794), 1 the corrected-matrix #if 0
+ * variant (kernel.cu:1435-1648) */
+int oracle_set_gradient(void* h, int32_t mode);
 int oracle_get_state(void* h, int8_t* typ, void* pos, void* vel, void* acc, void* prs,
                      void* pav);
 int oracle_set_state(void* h, const int8_t* typ, const void* pos, const void* vel,

@@ -34,6 +34,7 @@ SIGS = {
     "oracle_set_threads": (C.c_int, [C.c_int32]),
     "oracle_phase": (C.c_int, [C.c_void_p, C.c_int32]),
     "oracle_step": (C.c_int, [C.c_void_p, C.c_int32]),
+    "oracle_set_gradient": (C.c_int, [C.c_void_p, C.c_int32]),
     "oracle_get_state": (C.c_int, [C.c_void_p, c_int8_p] + [C.c_void_p] * 5),
     "oracle_set_state": (C.c_int, [C.c_void_p, c_int8_p] + [C.c_void_p] * 5),
     "oracle_get_wall_flags": (C.c_int, [C.c_void_p, c_int8_p]),
@@ -116,6 +117,10 @@ class Oracle:
 
     def step(self, n=1):
         assert lib().oracle_step(self.h, n) == 0
+
+    def set_gradient(self, mode: int):
+        """PrsGrdTrm variant: 0 as compiled, 1 the corrected-matrix #if 0 variant."""
+        assert lib().oracle_set_gradient(self.h, int(mode)) == 0
 
     def state(self):
         n, dt = self.n, self.dtype

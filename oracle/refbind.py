@@ -1,4 +1,4 @@
-"""ctypes binding of the reference's own kernels (oracle/_ref/libref_mps_{f32,f64}.so).
+"""ctypes binding of the reference's own kernels (oracle/_ref/libref_mps_*.so).
 
 TEST INFRASTRUCTURE. The libraries are built by ref_build.sh from the reference sources and
 run the reference's `class MPS` methods on the GPU. They exist only where that build ran;
@@ -22,18 +22,21 @@ PHASES = ["MkBkt", "Surface_Edge", "ResetMRR", "GenMRR_nonslip", "MkBkt_MRR", "V
 STEP_PHASES = [0, 2, 3, 4, 5, 6, 0, 7, 0, 8, 2, 3, 4, 9, 10]  # kernel.cu:1904-1935
 
 
-def path(precision: int) -> str:
-    return os.path.join(REF_DIR, "libref_mps_f64.so" if precision == 1 else "libref_mps_f32.so")
+def path(precision: int, corrected: bool = False) -> str:
+    """The build of the default kernels, or with ``corrected`` the one whose d_PrsGrdTrm is
+    the corrected-matrix variant (kernel.cu:1434-1648)."""
+    name = ("corr_" if corrected else "") + ("f64" if precision == 1 else "f32")
+    return os.path.join(REF_DIR, f"libref_mps_{name}.so")
 
 
-def available(precision: int = 0) -> bool:
-    return os.path.exists(path(precision))
+def available(precision: int = 0, corrected: bool = False) -> bool:
+    return os.path.exists(path(precision, corrected))
 
 
-def lib(precision: int):
-    key = 1 if precision == 1 else 0
+def lib(precision: int, corrected: bool = False):
+    key = (1 if precision == 1 else 0, bool(corrected))
     if key not in _libs:
-        L = C.CDLL(path(key))
+        L = C.CDLL(path(*key))
         L.ref_create.restype = C.c_void_p
         L.ref_create.argtypes = [C.c_void_p, C.c_int, c_int8_p, C.c_void_p, C.c_void_p, C.c_void_p]
         for nm in ("ref_phase", "ref_step"):
@@ -56,10 +59,10 @@ def _p(a):
 class Reference:
     """The reference solver on one scene (device memory is never freed by the reference)."""
 
-    def __init__(self, params, typ, pos, vel, nrm):
+    def __init__(self, params, typ, pos, vel, nrm, corrected: bool = False):
         self.precision = 1 if params.precision == 1 else 0
         self.dtype = np.float64 if self.precision == 1 else np.float32
-        self.L = lib(self.precision)
+        self.L = lib(self.precision, corrected)
         assert self.L.ref_real_size() == np.dtype(self.dtype).itemsize
         typ = np.ascontiguousarray(typ, np.int8)
         self.n = typ.shape[0]

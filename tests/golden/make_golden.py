@@ -8,7 +8,11 @@ particles (slot, position, pressure), and the bucket of every particle read back
 reference's linked lists. The CPU tests replay each method of the oracle from the recorded
 input state and compare with the recorded output state.
 
-    python tests/golden/make_golden.py [outdir]
+    python tests/golden/make_golden.py [outdir] [--corrected]
+
+With --corrected the same record is made with the reference's corrected-matrix d_PrsGrdTrm
+(the #if 0 variant, kernel.cu:1434-1648, built by oracle/ref_build.sh as libref_mps_corr_*)
+into ref_small_corr_{f32,f64}.npz.
 """
 from __future__ import annotations
 
@@ -46,14 +50,14 @@ def snapshot(ref, nf, tag, out):
     out[f"{tag}_cell"] = ref.buckets()
 
 
-def main(outdir: str):
+def main(outdir: str, corrected: bool = False):
     os.makedirs(outdir, exist_ok=True)
     for prec, name in ((0, "f32"), (1, "f64")):
         dty = np.float64 if prec == 1 else np.float32
         sc = dambreak(SCENE)
         p = dambreak_params(SCENE, dt=DT, precision=prec)
         args = (sc["typ"], sc["pos"].astype(dty), sc["vel"].astype(dty), sc["nrm"].astype(dty))
-        ref = refbind.Reference(p, *args)
+        ref = refbind.Reference(p, *args, corrected=corrected)
         nf = int(np.sum(sc["typ"] == 0))
         assert np.all(sc["typ"][:nf] == 0) and np.all(sc["typ"][nf:] != 0)
         out = {"params": params_array(p), "typ": sc["typ"], "pos": args[1], "vel": args[2],
@@ -71,10 +75,11 @@ def main(outdir: str):
                 ref.phase(ph)
                 if rec:
                     snapshot(ref, nf, f"s{step}_k{k + 1}", out)
-        path = os.path.join(outdir, f"ref_small_{name}.npz")
+        path = os.path.join(outdir, f"ref_small_{'corr_' if corrected else ''}{name}.npz")
         np.savez_compressed(path, **out)
         print(path, os.path.getsize(path))
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "tests", "golden"))
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    main(args[0] if args else os.path.join(ROOT, "tests", "golden"), "--corrected" in sys.argv)

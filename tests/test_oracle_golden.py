@@ -32,9 +32,10 @@ RTOL = {"f32": {"pos": 1e-6, "vel": 1e-5, "acc": 2e-4, "prs": 2e-4, "pav": 2e-4}
         "f64": {"pos": 1e-12, "vel": 1e-11, "acc": 1e-9, "prs": 1e-9, "pav": 1e-9}}
 
 
-def _oracle_at(g, tag):
+def _oracle_at(g, tag, gradient=0):
     p = golden_params(g)
     o = Oracle(p, g["typ"], g["pos"], g["vel"], g["nrm"])
+    o.set_gradient(gradient)
     o.set_wall_flags(g["wllse"])
     o.set_state(**golden_state(g, tag))
     o.set_mirrors(g[f"{tag}_mslot"], g[f"{tag}_mpos"], g[f"{tag}_mprs"])
@@ -87,21 +88,24 @@ def test_bucket_assignment_equals_reference(prec):
     assert n_checked == 6
 
 
-@pytest.mark.parametrize("prec", ["f32", "f64"])
+@pytest.mark.parametrize("prec", ["f32", "f64", "corr_f32", "corr_f64"])
 @pytest.mark.parametrize("phase", [5, 6, 7, 8, 9, 10])
 def test_method_matches_reference(prec, phase):
-    """VscTrm, UpPcl1, ChkCol, MkPrs, PrsGrdTrm, UpPcl2 from the reference's input state."""
+    """VscTrm, UpPcl1, ChkCol, MkPrs, PrsGrdTrm, UpPcl2 from the reference's input state.
+    corr_*: the reference built with its corrected-matrix PrsGrdTrm (the #if 0 variant,
+    kernel.cu:1434-1648), against the oracle's restatement of that variant."""
     g = golden(prec)
+    corrected = prec.startswith("corr_")
     nf = int(g["nf"])
     checked = 0
     for s, k, ph in _cases(prec):
         if ph != phase:
             continue
-        o = _oracle_at(g, f"s{s}_k{k}")
+        o = _oracle_at(g, f"s{s}_k{k}", 1 if corrected else 0)
         o.phase(ph)
         got, want = o.state(), golden_state(g, f"s{s}_k{k + 1}")
         assert np.array_equal(got["typ"], want["typ"])
-        for f, rt in RTOL[prec].items():
+        for f, rt in RTOL[prec.replace("corr_", "")].items():
             a = got[f][..., :nf].astype(np.float64)
             b = want[f][..., :nf].astype(np.float64)
             scale = max(np.abs(b).max(), 1e-30)

@@ -1,0 +1,91 @@
+"""bench.py's multi-rank plumbing on the CPU: two `gloo` ranks (no GPU needed).
+
+`bench.py --gpus N` runs one replica per GPU and reports the whole job's throughput from the
+slowest rank's device time (max over ranks). These tests run the same helpers as two
+processes over `gloo`: the process group comes up from the torchrun environment, the
+barrier returns on both ranks, the max reaches every rank, and a rank that never joins ends
+the other's collective with an error instead of a hang.
+"""
+from __future__ import annotations
+
+import multiprocessing as mp
+import os
+import socket
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _env(rank: int, world: int, port: int):
+    os.environ.update(WORLD_SIZE=str(world), RANK=str(rank), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), MPS_BENCH_BACKEND="gloo")
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+
+
+def _rank_main(rank: int, port: int, q):
+    _env(rank, 2, port)
+    import bench
+    import torch.distributed as dist
+    try:
+        world, r, local = bench.setup_dist()
+        bench.barrier(world)
+        # per-rank device time of K steps: the job is as fast as its slowest replica
+        ms = [120.0, 150.0][r]
+        worst = bench.allreduce_max(ms, world)
+        q.put((r, world, local, dist.get_backend(), worst))
+    finally:
+        dist.destroy_process_group()
+
+
+def _lonely_rank(port: int, q):
+    _env(0, 2, port)
+    import datetime
+
+    import torch.distributed as dist
+    try:
+        # the second rank never starts: the rendezvous must end with an error, not hang
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=3))
+        q.put("joined")
+    except Exception as e:  # noqa: BLE001 - any error is the expected outcome
+        q.put(type(e).__name__)
+
+
+def test_two_gloo_ranks_agree_on_the_slowest_rank():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_rank_main, args=(r, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(120)
+    assert all(p.exitcode == 0 for p in ps), [p.exitcode for p in ps]
+    got = sorted(q.get(timeout=5) for _ in range(2))
+    assert [g[0] for g in got] == [0, 1]
+    for r, world, local, backend, worst in got:
+        assert world == 2 and local == r and backend == "gloo"
+        assert worst == 150.0
+    # the bench's aggregate: every rank's particles over the slowest rank's time
+    nf, K = 384000, 200
+    assert 2 * nf * K / (150.0 / 1e3) == pytest.approx(1.024e9)
+
+
+def test_missing_rank_ends_with_an_error():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_lonely_rank, args=(_free_port(), q))
+    p.start()
+    p.join(120)
+    if p.is_alive():
+        p.kill()
+        pytest.fail("the rendezvous of a missing rank did not time out")
+    assert q.get(timeout=5) != "joined"

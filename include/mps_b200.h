@@ -243,6 +243,24 @@ int mps_set_stream(mps_handle* h, void* cuda_stream);
 int mps_set_option(mps_handle* h, int32_t option, int32_t value);
 int mps_synchronize(mps_handle* h);
 
+/*
+ * Moving walls. The reference declares a rotating wall (`w`, `wallangle`, `rot_rad`,
+ * class.cuh:117-121) and notes that Surface_Edge must run every step once walls move
+ * (kernel.cu:1879), but moves none: its OBJ/OBJ2 particles are static walls. This call gives
+ * every wall particle of `type` (MPS_OBJ or MPS_OBJ2) a prescribed rigid motion: rotation at
+ * `omega` rad/s about the line through `center` along `axis`, and translation at
+ * `velocity`; the centre moves with the walls. From the next mps_step on, each step ends by
+ * moving those walls one time step (positions, inward normals and the wall velocity that
+ * ChkCol uses, v + omega x r), rebuilding the wall buckets and rerunning Surface_Edge, so
+ * that the next step's mirrors and collisions see them at the new time. Mirrors keep the
+ * reference's zero velocity (kernel.cu:834-836). The motion accumulates in double from the
+ * walls' place when it is set; omega = 0 and velocity = 0 stop it (the walls stay where they
+ * are). mps_phase does not move walls. Single-scene handles only; the adjoint needs static
+ * walls. axis may be NULL when omega is 0.
+ */
+int mps_set_wall_motion(mps_handle* h, int32_t type, const double center[3],
+                        const double axis[3], double omega, const double velocity[3]);
+
 /* ---- time stepping ---------------------------------------------------------------- */
 
 /* Advance every scene by `nsteps` steps of the loop body kernel.cu:1904-1941. */

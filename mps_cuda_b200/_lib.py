@@ -128,6 +128,8 @@ SIGNATURES = {
     "mps_output_write": (C.c_int, [C.c_void_p, C.c_int32, C.c_double]),
     "mps_output_restart": (C.c_int, [C.c_void_p]),
     "mps_output_close": (C.c_int, [C.c_void_p]),
+    "mps_set_wall_motion": (C.c_int, [C.c_void_p, C.c_int32, c_double_p, c_double_p, C.c_double,
+                                      c_double_p]),
     "mps_status_string": (C.c_char_p, [C.c_int32]),
     "mps_last_error": (C.c_char_p, []),
 }

@@ -168,6 +168,11 @@ int mps_set_option(mps_handle* h, int32_t opt, int32_t value) {
     });
 }
 
+int mps_set_wall_motion(mps_handle* h, int32_t type, const double center[3],
+                        const double axis[3], double omega, const double velocity[3]) {
+    return guarded(h, [&](SolverBase& s) { s.set_wall_motion(type, center, axis, omega, velocity); });
+}
+
 int mps_synchronize(mps_handle* h) {
     return guarded(h, [&](SolverBase& s) { CK(cudaStreamSynchronize(s.stream)); });
 }

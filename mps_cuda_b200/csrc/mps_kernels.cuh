@@ -1151,6 +1151,65 @@ __global__ void k_ph_cull(PassArgs<R, RN> a) {
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// moving walls: the reference declares a rotating wall (w, wallangle, rot_rad,
+// class.cuh:117-121) and asks for Surface_Edge every step once walls move (kernel.cu:1879),
+// but never moves one. Here OBJ and OBJ2 can follow a prescribed rigid motion.
+// ---------------------------------------------------------------------------------------
+// q <- qs q and t <- t + vdt for every moving type (one thread, fixed operation order)
+static __global__ void k_motion_advance(WallMotion* m) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (int k = 0; k < 2; ++k) {
+        WallMotion& w = m[k];
+        if (w.type == 0) continue;
+        double r[9];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                r[3 * i + j] = (w.qs[3 * i] * w.q[j] + w.qs[3 * i + 1] * w.q[3 + j]) +
+                               w.qs[3 * i + 2] * w.q[6 + j];
+        for (int i = 0; i < 9; ++i) w.q[i] = r[i];
+        for (int d = 0; d < 3; ++d) w.t[d] = w.t[d] + w.vdt[d];
+    }
+}
+
+// the moving walls' place, normal and velocity from their reference state (x0, n0: double
+// SoA of the nW walls in load order)
+template <class R>
+__global__ void k_move_walls(const WallMotion* __restrict__ m, int nW,
+                             const int8_t* __restrict__ typ, const double* __restrict__ x0,
+                             const double* __restrict__ n0, V4<R>* pos, V4<R>* nrm, V4<R>* vel) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nW) return;
+    const int ty = typ[t];
+    const int k = (m[0].type != 0 && ty == m[0].type) ? 0 : ((m[1].type != 0 && ty == m[1].type) ? 1 : -1);
+    if (k < 0) return;
+    const WallMotion& w = m[k];
+    const double dx = x0[t] - w.c[0], dy = x0[nW + t] - w.c[1], dz = x0[2 * size_t(nW) + t] - w.c[2];
+    const double rx = (w.q[0] * dx + w.q[1] * dy) + w.q[2] * dz;
+    const double ry = (w.q[3] * dx + w.q[4] * dy) + w.q[5] * dz;
+    const double rz = (w.q[6] * dx + w.q[7] * dy) + w.q[8] * dz;
+    const double ax = n0[t], ay = n0[nW + t], az = n0[2 * size_t(nW) + t];
+    pos[t] = V4<R>{R((w.c[0] + w.t[0]) + rx), R((w.c[1] + w.t[1]) + ry), R((w.c[2] + w.t[2]) + rz),
+                   R(0)};
+    nrm[t] = V4<R>{R((w.q[0] * ax + w.q[1] * ay) + w.q[2] * az),
+                   R((w.q[3] * ax + w.q[4] * ay) + w.q[5] * az),
+                   R((w.q[6] * ax + w.q[7] * ay) + w.q[8] * az), R(0)};
+    vel[t] = V4<R>{R(w.v[0] + (w.w[1] * rz - w.w[2] * ry)), R(w.v[1] + (w.w[2] * rx - w.w[0] * rz)),
+                   R(w.v[2] + (w.w[0] * ry - w.w[1] * rx)), R(0)};
+}
+
+// reference state of the walls of one type, taken when its motion is set
+template <class R>
+__global__ void k_motion_snapshot(int nW, const int8_t* __restrict__ typ, int type,
+                                  const V4<R>* __restrict__ pos, const V4<R>* __restrict__ nrm,
+                                  double* x0, double* n0) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nW || typ[t] != type) return;
+    const V4<R> p = pos[t], n = nrm[t];
+    x0[t] = double(p.x); x0[nW + t] = double(p.y); x0[2 * size_t(nW) + t] = double(p.z);
+    n0[t] = double(n.x); n0[nW + t] = double(n.y); n0[2 * size_t(nW) + t] = double(n.z);
+}
+
 // d_Surface_Edge (kernel.cu:553-668) over the sorted walls
 template <class R, class RN>
 __global__ void k_surface_edge(const SceneDev<R, RN>* scs, int nscene, int nW, WallView<R> wl,

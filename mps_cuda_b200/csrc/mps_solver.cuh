@@ -201,6 +201,41 @@ template <class R> struct MirrorBuf {
     V4<R>* pos; int* slot;
 };
 
+// The motion of one wall type: the step's rotation by omega * dt about the unit axis
+// (Rodrigues' formula), the step's translation v * dt, and q = identity, t = 0.
+inline WallMotion wall_motion(int type, const double* c, const double* axis, double omega,
+                              const double* v, double dt) {
+    WallMotion w{};
+    double a[3] = {0.0, 0.0, 1.0};
+    if (omega != 0.0) {
+        const double nn = std::sqrt(axis[0] * axis[0] + axis[1] * axis[1] + axis[2] * axis[2]);
+        if (!(nn > 0.0) || !std::isfinite(nn))
+            throw ApiError(MPS_ERR_ARG, "the rotation axis must be a non-zero finite vector");
+        for (int d = 0; d < 3; ++d) a[d] = axis[d] / nn;
+    }
+    const double th = omega * dt, cs = std::cos(th), sn = std::sin(th), cc = 1.0 - cs;
+    const double qs[9] = {cs + a[0] * a[0] * cc, a[0] * a[1] * cc - a[2] * sn,
+                          a[0] * a[2] * cc + a[1] * sn, a[1] * a[0] * cc + a[2] * sn,
+                          cs + a[1] * a[1] * cc, a[1] * a[2] * cc - a[0] * sn,
+                          a[2] * a[0] * cc - a[1] * sn, a[2] * a[1] * cc + a[0] * sn,
+                          cs + a[2] * a[2] * cc};
+    bool moving = omega != 0.0;
+    for (int i = 0; i < 9; ++i) {
+        w.qs[i] = qs[i];
+        w.q[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    }
+    for (int d = 0; d < 3; ++d) {
+        w.c[d] = c[d];
+        w.t[d] = 0.0;
+        w.v[d] = v[d];
+        w.vdt[d] = v[d] * dt;
+        w.w[d] = omega * a[d];
+        moving = moving || v[d] != 0.0;
+    }
+    w.type = moving ? type : 0;
+    return w;
+}
+
 struct SolverBase {
     virtual ~SolverBase() {}
     int dev = 0;
@@ -237,6 +272,8 @@ struct SolverBase {
     virtual void output_snapshot(void* pos, void* vel, void* prs, void* pav, int8_t* typ,
                                  void* mpos, int* mslot, int* mcount_host) = 0;
     virtual void get_wall_normals(void* nrm) = 0;  // inward normals, SoA, id order
+    virtual void set_wall_motion(int type, const double* c, const double* axis, double omega,
+                                 const double* v) = 0;
     virtual void adjoint_record(int nsteps, int every) = 0;
     virtual void adjoint_backward(const double* lam_pos, const double* lam_vel, double* g_pos,
                                   double* g_vel, double* g_nu) = 0;
@@ -263,6 +300,13 @@ template <class R, class RN> class Solver final : public SolverBase {
     // walls, sorted once
     V4<R>* w_pos; V4<R>* w_nrm; V4<R>* w_vel; int* w_id; int8_t* w_typ; int8_t* w_se;
     int* wcs;
+    // walls in load order (the bucket build's source), and the moving walls' motion
+    V4<R>* tw_pos = nullptr; V4<R>* tw_vel = nullptr; V4<R>* tw_nrm = nullptr;
+    int8_t* tw_typ = nullptr; int* tw_id = nullptr;
+    double *mx0 = nullptr, *mn0 = nullptr;  // reference state of the moving walls
+    WallMotion* d_motion = nullptr;
+    WallMotion hmot[2] = {};
+    bool motion_on = false;
     // mirrors: raw list U and two sorted generations
     MirrorBuf<R> U, M1, M2;
     int *mcs1, *mcs2;
@@ -444,29 +488,19 @@ template <class R, class RN> class Solver final : public SolverBase {
         if (nW > 0) {
             // walls: unsorted copy in id order, then one bucket build into w_*
             V4<R>* sp = ar.template get<V4<R>>(3 * size_t(nW));
-            V4<R>* tw_pos = sp;
-            V4<R>* tw_vel = sp + nW;
-            V4<R>* tw_nrm = sp + 2 * size_t(nW);
-            int8_t* tw_typ = ar.template get<int8_t>(nW);
-            int* tw_id = ar.template get<int>(nW);
+            tw_pos = sp;
+            tw_vel = sp + nW;
+            tw_nrm = sp + 2 * size_t(nW);
+            tw_typ = ar.template get<int8_t>(nW);
+            tw_id = ar.template get<int>(nW);
             k_load_walls<R><<<blocks(nW, 256), 256, 0, stream>>>(nT, io.pos, io.vel, io.acc, io.typ,
                                                                  d_wall_ids, nW, tw_pos, tw_vel,
                                                                  tw_nrm, tw_id, tw_typ);
             KL();
-            WallKeySrc<R, RN> ks{d_sc, nscene, dead(), tw_pos, tw_id};
-            WallGather<R> g{tw_pos, tw_nrm, tw_vel, tw_id, tw_typ, w_pos, w_nrm, w_vel, w_id, w_typ};
-            bin(ks, g, nullptr, nW, wcs, L());
-            WallView<R> wl = wall_view();
-            k_surface_edge<R, RN><<<blocks(nW, 128), 128, 0, stream>>>(d_sc, nscene, nW, wl, w_id,
-                                                                       w_se);
-            KL();
+            bin_walls();
         } else {
             CK(cudaMemsetAsync(wcs, 0, sizeof(int) * (L() + 1), stream));
-        }
-        {
-            dim3 g(std::max(1, std::min(blocks(C, 256), 148 * 4)), nscene);
-            k_near_wall<R, RN><<<g, 256, 0, stream>>>(d_sc, nscene, wcs, near_wall);
-            KL();
+            near_wall_flags();
         }
         load_fluid(false);
         mkbkt(true);
@@ -647,6 +681,61 @@ template <class R, class RN> class Solver final : public SolverBase {
     }
 
 
+    // wall bucket build from the load-order copy, then Surface_Edge (kernel.cu:553-668) and
+    // the near-wall flags of every bucket
+    void bin_walls() {
+        WallKeySrc<R, RN> ks{d_sc, nscene, dead(), tw_pos, tw_id};
+        WallGather<R> g{tw_pos, tw_nrm, tw_vel, tw_id, tw_typ, w_pos, w_nrm, w_vel, w_id, w_typ};
+        bin(ks, g, nullptr, nW, wcs, L());
+        k_surface_edge<R, RN><<<blocks(nW, 128), 128, 0, stream>>>(d_sc, nscene, nW, wall_view(),
+                                                                   w_id, w_se);
+        KL();
+        near_wall_flags();
+    }
+
+    void near_wall_flags() {
+        dim3 g(std::max(1, std::min(blocks(C, 256), 148 * 4)), nscene);
+        k_near_wall<R, RN><<<g, 256, 0, stream>>>(d_sc, nscene, wcs, near_wall);
+        KL();
+    }
+
+    // one step of the moving walls, then their buckets, edge flags and near-wall flags
+    void move_walls() {
+        k_motion_advance<<<1, 1, 0, stream>>>(d_motion);
+        KL();
+        k_move_walls<R><<<blocks(nW, 256), 256, 0, stream>>>(d_motion, nW, tw_typ, mx0, mn0, tw_pos,
+                                                             tw_nrm, tw_vel);
+        KL();
+        bin_walls();
+    }
+
+    void set_wall_motion(int type, const double* c, const double* axis, double omega,
+                         const double* v) override {
+        if (type != kOBJ && type != kOBJ2)
+            throw ApiError(MPS_ERR_ARG, "only MPS_OBJ and MPS_OBJ2 walls move");
+        if (nscene != 1)
+            throw ApiError(MPS_ERR_UNSUPPORTED, "wall motion needs a single-scene handle");
+        if (!c || !v || (omega != 0.0 && !axis))
+            throw ApiError(MPS_ERR_ARG, "centre and velocity (and the axis of a rotation) are needed");
+        WallMotion w = wall_motion(type, c, axis, omega, v, double(hsc[0].dt));
+        if (!d_motion) {
+            d_motion = ar.template get<WallMotion>(2);
+            mx0 = ar.template get<double>(3 * size_t(std::max(nW, 1)));
+            mn0 = ar.template get<double>(3 * size_t(std::max(nW, 1)));
+        }
+        const int k = type == kOBJ ? 0 : 1;
+        if (w.type != 0 && nW > 0) {
+            k_motion_snapshot<R><<<blocks(nW, 256), 256, 0, stream>>>(nW, tw_typ, type, tw_pos,
+                                                                      tw_nrm, mx0, mn0);
+            KL();
+        }
+        hmot[k] = w;
+        CK(cudaMemcpyAsync(d_motion, hmot, sizeof(hmot), cudaMemcpyHostToDevice, stream));
+        CK(cudaStreamSynchronize(stream));
+        motion_on = nW > 0 && (hmot[0].type != 0 || hmot[1].type != 0);
+        invalidate_graph();
+    }
+
     template <bool D> void fused_body() {
         const int ba = blk[MPS_K_PASS_A], bb = blk[MPS_K_PASS_B], bc = blk[MPS_K_PASS_C],
                   bg = blk[MPS_K_GEN];
@@ -683,6 +772,8 @@ template <class R, class RN> class Solver final : public SolverBase {
                 k_pass_c<R, RN, D><<<blocks(nF, bc), bc, 0, stream>>>(args(M2, mcs2));
             KL();
         }
+        // walls that move take their place at the new time before the next step's mirrors
+        if (motion_on) move_walls();
         reset_raw();
         {
             Scope t(this, MPS_K_GEN);
@@ -1144,6 +1235,8 @@ template <class R, class RN> class Solver final : public SolverBase {
         if (grad_mode != MPS_GRAD_STANDARD)
             throw ApiError(MPS_ERR_UNSUPPORTED,
                            "the adjoint covers the default PrsGrdTrm only (MPS_GRAD_STANDARD)");
+        if (motion_on)
+            throw ApiError(MPS_ERR_UNSUPPORTED, "the adjoint needs static walls");
         if (nscene != 1)
             throw ApiError(MPS_ERR_UNSUPPORTED, "the adjoint runs on single-scene handles");
         if (nsteps <= 0 || every <= 0)

@@ -58,6 +58,21 @@ template <class R, class RN> struct SceneDev {
     RN rp_n;
 };
 
+// Prescribed rigid motion of one moving-wall type (OBJ or OBJ2), in double: a wall particle
+// set moving at x0 with normal n0 is at c + t + q (x0 - c) with normal q n0 and velocity
+// v + w x (q (x0 - c)), where q and t accumulate one step's rotation qs and translation vdt.
+struct WallMotion {
+    double qs[9];   // rotation of one step, row-major
+    double q[9];    // rotation since the motion was set
+    double c[3];    // centre of rotation when the motion was set
+    double t[3];    // translation since the motion was set
+    double vdt[3];  // translation of one step
+    double w[3];    // angular velocity vector
+    double v[3];    // translation velocity
+    int type;       // particle type that moves (kOBJ or kOBJ2), 0 when off
+    int pad;
+};
+
 struct DevCounters {
     int mirror_raw;       // entries appended to the raw mirror list
     int err_mirror_slot;  // corner mirror without a free slot (kernel.cu:868-874)

@@ -160,6 +160,16 @@ class MPSBatch:
     def synchronize(self):
         check(lib().mps_synchronize(self._h), "mps_synchronize")
 
+    def set_wall_motion(self, typ: int, center, axis=None, omega: float = 0.0,
+                        velocity=(0.0, 0.0, 0.0)):
+        """Prescribed rigid motion of every wall of type `typ` (OBJ or OBJ2): rotation at
+        omega rad/s about the line through `center` along `axis`, translation at `velocity`."""
+        c = (C.c_double * 3)(*[float(x) for x in center])
+        a = None if axis is None else (C.c_double * 3)(*[float(x) for x in axis])
+        v = (C.c_double * 3)(*[float(x) for x in velocity])
+        check(lib().mps_set_wall_motion(self._h, int(typ), c, a, float(omega), v),
+              "mps_set_wall_motion")
+
     # -- stepping ----------------------------------------------------------------------
     def step(self, n: int = 1):
         check(lib().mps_step(self._h, int(n)), "mps_step")

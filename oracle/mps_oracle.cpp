@@ -81,6 +81,14 @@ struct Oracle {
     RN n0_grad_n, prs_coef_n, pmax_n, rho_n;
     R rlim2, col, rho, knm, snd, prs_coef, pmax, umax, dt, rlim_wall2, edge_r2;
     int grad_mode = 0;  // 0: PrsGrdTrm as compiled (kernel.cu:1651-1794), 1: the #if 0 variant
+    // prescribed motion of OBJ (0) and OBJ2 (1) walls: a wall set moving at x0 with normal n0
+    // is at c + t + q (x0 - c), normal q n0, velocity v + w x (q (x0 - c)); q and t gather
+    // one step's rotation qs (omega dt about the unit axis, Rodrigues) and translation v dt
+    struct Motion {
+        int type = 0;
+        double qs[9], q[9], c[3], t[3], vdt[3], w[3], v[3];
+    } mot[2];
+    std::vector<double> mx0, mn0;  // reference state of moving walls, SoA by particle id
 
     int n;
     std::vector<int8_t> typ, wse;
@@ -642,6 +650,86 @@ struct Oracle {
         }
     }
 
+    // ---- moving walls ---------------------------------------------------------------------
+    int set_motion(int type, const double* c, const double* axis, double omega, const double* v) {
+        if (type != OBJ && type != OBJ2) return 1;
+        Motion w;
+        double a[3] = {0.0, 0.0, 1.0};
+        if (omega != 0.0) {
+            const double nn = std::sqrt(axis[0] * axis[0] + axis[1] * axis[1] + axis[2] * axis[2]);
+            if (!(nn > 0.0)) return 1;
+            for (int d = 0; d < 3; ++d) a[d] = axis[d] / nn;
+        }
+        const double step = double(dt);
+        const double th = omega * step, cs = std::cos(th), sn = std::sin(th), cc = 1.0 - cs;
+        const double qs[9] = {cs + a[0] * a[0] * cc, a[0] * a[1] * cc - a[2] * sn,
+                              a[0] * a[2] * cc + a[1] * sn, a[1] * a[0] * cc + a[2] * sn,
+                              cs + a[1] * a[1] * cc, a[1] * a[2] * cc - a[0] * sn,
+                              a[2] * a[0] * cc - a[1] * sn, a[2] * a[1] * cc + a[0] * sn,
+                              cs + a[2] * a[2] * cc};
+        bool moving = omega != 0.0;
+        for (int i = 0; i < 9; ++i) {
+            w.qs[i] = qs[i];
+            w.q[i] = (i % 4 == 0) ? 1.0 : 0.0;
+        }
+        for (int d = 0; d < 3; ++d) {
+            w.c[d] = c[d];
+            w.t[d] = 0.0;
+            w.v[d] = v[d];
+            w.vdt[d] = v[d] * step;
+            w.w[d] = omega * a[d];
+            moving = moving || v[d] != 0.0;
+        }
+        w.type = moving ? type : 0;
+        if (mx0.empty()) {
+            mx0.assign(3 * size_t(n), 0.0);
+            mn0.assign(3 * size_t(n), 0.0);
+        }
+        if (w.type != 0)
+            for (int i = 0; i < n; ++i)
+                if (typ[i] == type) {
+                    mx0[i] = double(px[i]); mx0[n + i] = double(py[i]); mx0[2 * size_t(n) + i] = double(pz[i]);
+                    mn0[i] = double(nx[i]); mn0[n + i] = double(ny[i]); mn0[2 * size_t(n) + i] = double(nz[i]);
+                }
+        mot[type == OBJ ? 0 : 1] = w;
+        return 0;
+    }
+
+    bool moving() const { return mot[0].type != 0 || mot[1].type != 0; }
+
+    void move_walls() {
+        for (Motion& w : mot) {
+            if (w.type == 0) continue;
+            double r[9];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j)
+                    r[3 * i + j] = (w.qs[3 * i] * w.q[j] + w.qs[3 * i + 1] * w.q[3 + j]) +
+                                   w.qs[3 * i + 2] * w.q[6 + j];
+            for (int i = 0; i < 9; ++i) w.q[i] = r[i];
+            for (int d = 0; d < 3; ++d) w.t[d] = w.t[d] + w.vdt[d];
+        }
+        for (int i = 0; i < n; ++i) {
+            const int k = (mot[0].type != 0 && typ[i] == mot[0].type)
+                              ? 0 : ((mot[1].type != 0 && typ[i] == mot[1].type) ? 1 : -1);
+            if (k < 0) continue;
+            const Motion& w = mot[k];
+            const double dx = mx0[i] - w.c[0], dy = mx0[n + i] - w.c[1], dz = mx0[2 * size_t(n) + i] - w.c[2];
+            const double rx = (w.q[0] * dx + w.q[1] * dy) + w.q[2] * dz;
+            const double ry = (w.q[3] * dx + w.q[4] * dy) + w.q[5] * dz;
+            const double rz = (w.q[6] * dx + w.q[7] * dy) + w.q[8] * dz;
+            const double ax = mn0[i], ay = mn0[n + i], az = mn0[2 * size_t(n) + i];
+            px[i] = R((w.c[0] + w.t[0]) + rx);
+            py[i] = R((w.c[1] + w.t[1]) + ry);
+            pz[i] = R((w.c[2] + w.t[2]) + rz);
+            nx[i] = R((w.q[0] * ax + w.q[1] * ay) + w.q[2] * az);
+            ny[i] = R((w.q[3] * ax + w.q[4] * ay) + w.q[5] * az);
+            nz[i] = R((w.q[6] * ax + w.q[7] * ay) + w.q[8] * az);
+            vx[i] = R(w.v[0] + (w.w[1] * rz - w.w[2] * ry));
+            vy[i] = R(w.v[1] + (w.w[2] * rx - w.w[0] * rz));
+            vz[i] = R(w.v[2] + (w.w[0] * ry - w.w[1] * rx));
+        }
+    }
+
     // ---- PrsGrdTrm, corrected-matrix variant (the #if 0 branch, kernel.cu:1435-1648) -------
     // P_min as in the active variant; then the moment matrix sum w r r^T (nine sums, each
     // row a times column b as (w r_a) r_b) and the right side sum w (P_j - P_min) r over the
@@ -827,6 +915,11 @@ struct Oracle {
         reset_mrr(); gen_mrr(); mkbkt_mrr_phase();
         prsgrdtrm();
         uppcl2();
+        if (moving()) {  // walls take their place at the new time, with their edge flags
+            move_walls();
+            mkbkt();
+            surface_edge();
+        }
     }
 };
 
@@ -916,6 +1009,12 @@ int oracle_set_gradient(void* h, int32_t mode) {
         o.grad_mode = mode;
         return 0;
     });
+}
+
+int oracle_set_wall_motion(void* h, int32_t type, const double* center, const double* axis,
+                           double omega, const double* velocity) {
+    if (!center || !velocity || (omega != 0.0 && !axis)) return 1;
+    return dispatch(h, [&](auto& o) { return o.set_motion(type, center, axis, omega, velocity); });
 }
 
 int oracle_step(void* h, int32_t k) {

@@ -35,6 +35,10 @@ int oracle_step(void* h, int32_t nsteps);
 /* PrsGrdTrm variant: 0 as compiled (kernel.cu:1651-1794), 1 the corrected-matrix #if 0
  * variant (kernel.cu:1435-1648) */
 int oracle_set_gradient(void* h, int32_t mode);
+/* prescribed rigid motion of the OBJ / OBJ2 walls, applied at the end of every step (the
+ * same motion as mps_set_wall_motion) */
+int oracle_set_wall_motion(void* h, int32_t type, const double* center, const double* axis,
+                           double omega, const double* velocity);
 int oracle_get_state(void* h, int8_t* typ, void* pos, void* vel, void* acc, void* prs,
                      void* pav);
 int oracle_set_state(void* h, const int8_t* typ, const void* pos, const void* vel,

@@ -35,6 +35,8 @@ SIGS = {
     "oracle_phase": (C.c_int, [C.c_void_p, C.c_int32]),
     "oracle_step": (C.c_int, [C.c_void_p, C.c_int32]),
     "oracle_set_gradient": (C.c_int, [C.c_void_p, C.c_int32]),
+    "oracle_set_wall_motion": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double)]),
     "oracle_get_state": (C.c_int, [C.c_void_p, c_int8_p] + [C.c_void_p] * 5),
     "oracle_set_state": (C.c_int, [C.c_void_p, c_int8_p] + [C.c_void_p] * 5),
     "oracle_get_wall_flags": (C.c_int, [C.c_void_p, c_int8_p]),
@@ -117,6 +119,13 @@ class Oracle:
 
     def step(self, n=1):
         assert lib().oracle_step(self.h, n) == 0
+
+    def set_wall_motion(self, typ: int, center, axis=None, omega: float = 0.0,
+                        velocity=(0.0, 0.0, 0.0)):
+        c = (C.c_double * 3)(*[float(x) for x in center])
+        a = None if axis is None else (C.c_double * 3)(*[float(x) for x in axis])
+        v = (C.c_double * 3)(*[float(x) for x in velocity])
+        assert lib().oracle_set_wall_motion(self.h, int(typ), c, a, float(omega), v) == 0
 
     def set_gradient(self, mode: int):
         """PrsGrdTrm variant: 0 as compiled, 1 the corrected-matrix #if 0 variant."""

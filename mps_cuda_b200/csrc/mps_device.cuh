@@ -570,15 +570,46 @@ template <class R> struct MirrorPlan {
     R sx, sy, sz;  // normalised sum of the distinct Edge normals
 };
 
+// A set of up to kNumMRR distinct normals in arrival order; the first three live in
+// registers (walls meet a particle from one to three planes), the rest in a local array.
+template <class R> struct NormalSet {
+    int n = 0;
+    R ax = R(0), ay = R(0), az = R(0), bx = R(0), by = R(0), bz = R(0), cx = R(0), cy = R(0),
+      cz = R(0);
+    R rest[kNumMRR - 3][3];
+    __device__ __forceinline__ bool has(R x, R y, R z) const {
+        if (n > 0 && ax == x && ay == y && az == z) return true;
+        if (n > 1 && bx == x && by == y && bz == z) return true;
+        if (n > 2 && cx == x && cy == y && cz == z) return true;
+        for (int k = 3; k < n; ++k)
+            if (rest[k - 3][0] == x && rest[k - 3][1] == y && rest[k - 3][2] == z) return true;
+        return false;
+    }
+    __device__ __forceinline__ void add(R x, R y, R z) {
+        if (n == 0) { ax = x; ay = y; az = z; }
+        else if (n == 1) { bx = x; by = y; bz = z; }
+        else if (n == 2) { cx = x; cy = y; cz = z; }
+        else { rest[n - 3][0] = x; rest[n - 3][1] = y; rest[n - 3][2] = z; }
+        ++n;
+    }
+    // component sums in arrival order
+    __device__ __forceinline__ void sum(R& sx, R& sy, R& sz) const {
+        sx = R(0); sy = R(0); sz = R(0);
+        if (n > 0) { sx += ax; sy += ay; sz += az; }
+        if (n > 1) { sx += bx; sy += by; sz += bz; }
+        if (n > 2) { sx += cx; sy += cy; sz += cz; }
+        for (int k = 3; k < n; ++k) { sx += rest[k - 3][0]; sy += rest[k - 3][1]; sz += rest[k - 3][2]; }
+    }
+};
+
 // registration (kernel.cu:741-800): every distinct normal once, the first wall found wins;
 // Edge walls likewise. Returns the number of walls inside r (diagnostic).
 template <class R, class RN>
 __device__ __forceinline__ int plan_mirrors(const SceneDev<R, RN>& sc, const RowCtx<R>& c, R x,
                                             R y, R z, const WallView<R>& wl, bool skip,
                                             MirrorPlan<R>& pl) {
-    int edg[kNumMRR];
-    R rn[kNumMRR][3], en[kNumMRR][3];
-    int nreg = 0, nedge = 0, nwall = 0;
+    NormalSet<R> reg, edge;
+    int last_edge = -1, nwall = 0;
     for_rows(sc, wl.cs, c, skip ? sc.skip_r : R(INFINITY), [&](int j) {
         V4<R> q = ldg4(wl.pos + j);
         R dx = x - q.x, dy = y - q.y, dz = z - q.z;
@@ -586,36 +617,24 @@ __device__ __forceinline__ int plan_mirrors(const SceneDev<R, RN>& sc, const Row
         if (!(d2 <= sc.r2)) return;
         ++nwall;
         V4<R> nv = ldg4(wl.nrm + j);
-        bool dup = false;
-        for (int k = 0; k < nreg; ++k)
-            if (rn[k][0] == nv.x && rn[k][1] == nv.y && rn[k][2] == nv.z) dup = true;
-        if (!dup && nreg < kNumMRR) {
-            pl.reg[nreg] = j;
-            rn[nreg][0] = nv.x; rn[nreg][1] = nv.y; rn[nreg][2] = nv.z;
-            ++nreg;
+        if (reg.n < kNumMRR && !reg.has(nv.x, nv.y, nv.z)) {
+            pl.reg[reg.n] = j;
+            reg.add(nv.x, nv.y, nv.z);
         }
-        if (__ldg(wl.wse + j) == kEDGE) {
-            bool edup = false;
-            for (int k = 0; k < nedge; ++k)
-                if (en[k][0] == nv.x && en[k][1] == nv.y && en[k][2] == nv.z) edup = true;
-            if (!edup && nedge < kNumMRR) {
-                edg[nedge] = j;
-                en[nedge][0] = nv.x; en[nedge][1] = nv.y; en[nedge][2] = nv.z;
-                ++nedge;
-            }
+        if (__ldg(wl.wse + j) == kEDGE && edge.n < kNumMRR && !edge.has(nv.x, nv.y, nv.z)) {
+            last_edge = j;
+            edge.add(nv.x, nv.y, nv.z);
         }
     });
-    pl.nreg = nreg;
+    pl.nreg = reg.n;
     pl.corner = -1;
     // corner mirror through the last Edge wall (kernel.cu:841-858)
-    if (nreg > 0 && nedge >= 2) {
-        R sx = 0, sy = 0, sz = 0;
-        for (int k = 0; k < nedge; ++k) {
-            sx += en[k][0]; sy += en[k][1]; sz += en[k][2];
-        }
+    if (reg.n > 0 && edge.n >= 2) {
+        R sx, sy, sz;
+        edge.sum(sx, sy, sz);
         R as = sqrtR(dot3(sx, sy, sz, sx, sy, sz));
         pl.sx = sx / as; pl.sy = sy / as; pl.sz = sz / as;
-        pl.corner = edg[nedge - 1];
+        pl.corner = last_edge;
     }
     return nwall;
 }

@@ -84,9 +84,28 @@ __device__ __forceinline__ int item_count(const int* n_ptr, int n_fixed) {
     return n_ptr ? min(*n_ptr, n_fixed) : n_fixed;
 }
 
+constexpr int kScan16Threads = 512, kScan16Per = 16, kScan16Tile = kScan16Threads * kScan16Per;
+
+// Adds each lane's item to part[tile] (tile < 0: no item), one atomic per run of lanes with
+// the same tile: items arrive nearly sorted by bucket (a warp's mirrors come from
+// neighbouring particles), so a warp's tiles form a few runs. Every lane of the warp calls
+// this.
+__device__ __forceinline__ void tile_runs_add(int tile, int lane, int* __restrict__ part) {
+    const int prev = __shfl_up_sync(0xffffffffu, tile, 1);
+    const bool start = lane == 0 || tile != prev;
+    const unsigned starts = __ballot_sync(0xffffffffu, start);
+    if (start && tile >= 0) {
+        const unsigned later = starts & ~((2u << lane) - 1u);
+        const int end = later ? __ffs(later) - 1 : 32;
+        atomicAdd(&part[tile], end - lane);
+    }
+}
+
 template <class Src>
 __global__ void k_bin_key(Src src, const int* n_ptr, int n_fixed, int* __restrict__ key,
-                          int* __restrict__ rnk, int* __restrict__ count, DevCounters* cnt) {
+                          int* __restrict__ rnk, int* __restrict__ count, int* __restrict__ part,
+                          DevCounters* cnt) {
+    // part (may be null): per kScan16Tile tile totals of count, for k_fine_scan
     const int n = item_count(n_ptr, n_fixed);
     const int lane = threadIdx.x & 31;
     const int stride = gridDim.x * blockDim.x;
@@ -100,6 +119,7 @@ __global__ void k_bin_key(Src src, const int* n_ptr, int n_fixed, int* __restric
         int below = __popc(peers & ((1u << lane) - 1));
         int b = 0;
         if (act && lane == leader) b = atomicAdd(&count[c], __popc(peers));
+        if (part) tile_runs_add(act ? c / kScan16Tile : -1, lane, part);  // uniform branch
         b = __shfl_sync(0xffffffffu, b, leader);
         if (act) {
             key[t] = c;
@@ -108,41 +128,32 @@ __global__ void k_bin_key(Src src, const int* n_ptr, int n_fixed, int* __restric
     }
 }
 
-constexpr int kScan16Threads = 512, kScan16Per = 16, kScan16Tile = kScan16Threads * kScan16Per;
 
-// k_bin_key for the fluid: counts each fine cell's items at its bucket-major index (count)
-// and at its row-major index (count_r), and adds every item to the total of its scan tile
-// (kScan16Tile cells) in both orders (part, part_r), so that k_fine_scan needs no reduce pass.
-// The tile totals take one atomic per tile a warp touches.
+// k_bin_key for the fluid: also counts each fine cell's items at its row-major index
 template <class R, class RN>
 __global__ void k_bin_key_fluid(FluidKeySrc<R, RN> src, int n, int* __restrict__ key,
                                 int* __restrict__ rnk, int* __restrict__ count,
-                                int* __restrict__ count_r, int* __restrict__ part,
-                                int* __restrict__ part_r, DevCounters* cnt) {
+                                int* __restrict__ count_r, DevCounters* cnt) {
     const int lane = threadIdx.x & 31;
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
-        const int t = base + lane;
-        const bool act = t < n;
-        const int c = act ? src.key(t, cnt) : -1;
-        int cr = c;
-        if (act && c != src.dead) {
-            const SceneDev<R, RN>& s =
-                src.sc[src.nscene > 1 ? scene_of(src.sc, src.nscene, src.pid[t]) : 0];
-            cr = fine_rowmajor(s, c);
-        }
-        const unsigned peers = __match_any_sync(0xffffffffu, c);
-        const int leader = __ffs(peers) - 1;
-        const int below = __popc(peers & ((1u << lane) - 1));
+        int t = base + lane;
+        bool act = t < n;
+        int c = act ? src.key(t, cnt) : -1;
+        unsigned peers = __match_any_sync(0xffffffffu, c);
+        int leader = __ffs(peers) - 1;
+        int below = __popc(peers & ((1u << lane) - 1));
         int b = 0;
         if (act && lane == leader) {
             b = atomicAdd(&count[c], __popc(peers));
+            int cr = c;
+            if (c != src.dead) {
+                const SceneDev<R, RN>& s =
+                    src.sc[src.nscene > 1 ? scene_of(src.sc, src.nscene, src.pid[t]) : 0];
+                cr = fine_rowmajor(s, c);
+            }
             atomicAdd(&count_r[cr], __popc(peers));
         }
-        const unsigned tf = __match_any_sync(0xffffffffu, act ? c / kScan16Tile : -1);
-        const unsigned tr = __match_any_sync(0xffffffffu, act ? cr / kScan16Tile : -1);
-        if (act && lane == __ffs(tf) - 1) atomicAdd(&part[c / kScan16Tile], __popc(tf));
-        if (act && lane == __ffs(tr) - 1) atomicAdd(&part_r[cr / kScan16Tile], __popc(tr));
         b = __shfl_sync(0xffffffffu, b, leader);
         if (act) {
             key[t] = c;
@@ -356,8 +367,9 @@ __device__ __forceinline__ void load16(const int* __restrict__ in, int base, int
     }
 }
 
-// The two fine-cell tables of a fluid bucket build: count[k] (k = 0: bucket-major, 1:
-// row-major) with its per-tile totals part[k] from k_bin_key_fluid, scanned into out[k].
+// Count tables of a bucket build with their per-tile totals (from the key kernel, or from
+// k_fine_tile_sums): the fluid build's two fine-cell tables (k = 0: bucket-major, 1:
+// row-major), or one bucket table (gridDim.y = 1), count[k] scanned into out[k].
 struct FineScan {
     int* count[2];
     int* part[2];
@@ -366,9 +378,21 @@ struct FineScan {
     int* ticket;  // blocks finished; zero between launches
 };
 
+// part[k][b] = sum of count[k] over tile b (kScan16Tile entries), for k = blockIdx.y
+static __global__ void __launch_bounds__(kScan16Threads) k_fine_tile_sums(FineScan f) {
+    __shared__ int sh[32];
+    int v[16];
+    load16(f.count[blockIdx.y], blockIdx.x * kScan16Tile + threadIdx.x * kScan16Per, f.L, v);
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) s += v[k];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) f.part[blockIdx.y][blockIdx.x] = s;
+}
+
 // Exclusive scan of count[k][0..L) into out[k][0..L], out[k][L] = total, for k = blockIdx.y.
 // The counts are left zero; the last block to finish also zeroes the tile totals for the
-// next build (every block has read them by then).
+// next build (every block has read them by then), so a build needs no memset.
 static __global__ void __launch_bounds__(kScan16Threads) k_fine_scan(FineScan f) {
     __shared__ int sh[32];
     __shared__ int wsum[32];
@@ -434,10 +458,8 @@ static __global__ void __launch_bounds__(kScan16Threads) k_fine_scan(FineScan f)
     }
     __syncthreads();
     if (last) {
-        for (int k = threadIdx.x; k < f.ntile; k += blockDim.x) {
-            f.part[0][k] = 0;
-            f.part[1][k] = 0;
-        }
+        for (int k = threadIdx.x; k < f.ntile; k += blockDim.x)
+            for (int y = 0; y < int(gridDim.y); ++y) f.part[y][k] = 0;
         if (threadIdx.x == 0) *f.ticket = 0;
     }
 }

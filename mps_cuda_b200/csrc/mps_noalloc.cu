@@ -114,7 +114,7 @@ int run(const mps_params& p, int n, const int8_t* typ, const void* pos, int32_t*
     const int nb = (L + kScanTile - 1) / kScanTile;
     // counters start at zero: the array still holds the previous call's values
     k_zero<<<gc, 256, 0, st>>>(count, L);
-    if (n > 0) k_bin_key<SoaKeySrc<R>><<<gi, 256, 0, st>>>(src, nullptr, n, key, rnk, count, nullptr);
+    if (n > 0) k_bin_key<SoaKeySrc<R>><<<gi, 256, 0, st>>>(src, nullptr, n, key, rnk, count, nullptr, nullptr);
     k_scan_reduce<<<nb, kScanThreads, 0, st>>>(count, L, part);
     k_scan_apply<<<nb, kScanThreads, 0, st>>>(count, L, part, cs);
     if (n > 0) {

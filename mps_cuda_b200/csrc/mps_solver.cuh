@@ -314,7 +314,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     // fluid positions in row-major fine-cell order (slot in w) and that order's cell starts
     V4<R>* posf;
     int *csr, *count_f, *count_r;
-    int *part_f, *part_r;  // per scan tile totals of count_f / count_r (k_bin_key_fluid)
+    int *part_f, *part_r;  // per scan tile totals of count_f / count_r (k_fine_tile_sums)
     bool posf_stale = false;  // particles moved in place since the copy was made
     // bucket-build scratch
     int *key, *rnk, *seg, *count, *part;
@@ -555,7 +555,9 @@ template <class R, class RN> class Solver final : public SolverBase {
         rnk = ar.template get<int>(items);
         seg = ar.template get<int>(items);
         count = ar.template get<int>(L());
-        part = ar.template get<int>((L() + kScanTile - 1) / kScanTile + 1);
+        part = ar.template get<int>((L() + kScan16Tile - 1) / kScan16Tile + 1);
+        CK(cudaMemsetAsync(count, 0, sizeof(int) * L(), stream));
+        CK(cudaMemsetAsync(part, 0, sizeof(int) * ((L() + kScan16Tile - 1) / kScan16Tile + 1), stream));
         d_fluid_ids = ar.template get<int>(F);
         d_wall_ids = ar.template get<int>(W);
         d_nF = ar.template get<int>(1);
@@ -584,17 +586,16 @@ template <class R, class RN> class Solver final : public SolverBase {
     // ---- bucket build ------------------------------------------------------------------
     // bucket build over `ncell` cells (the last one, `ncell - 1`, holds unlisted items)
     template <class Src, class G>
+    // (count and part are zero between builds: the scan clears them)
     void bin(Src src, G g, const int* n_ptr, int n_max, int* out_cs, int ncell) {
-        CK(cudaMemsetAsync(count, 0, sizeof(int) * size_t(ncell), stream));
         if (n_max > 0) {
             int grid = std::min(blocks(n_max, 256), 148 * 32);
-            k_bin_key<Src><<<grid, 256, 0, stream>>>(src, n_ptr, n_max, key, rnk, count, cnt);
+            k_bin_key<Src><<<grid, 256, 0, stream>>>(src, n_ptr, n_max, key, rnk, count, part, cnt);
             KL();
         }
-        int nb = (ncell + kScanTile - 1) / kScanTile;
-        k_scan_reduce<<<nb, kScanThreads, 0, stream>>>(count, ncell, part);
-        KL();
-        k_scan_apply<<<nb, kScanThreads, 0, stream>>>(count, ncell, part, out_cs);
+        const int nb = (ncell + kScan16Tile - 1) / kScan16Tile;
+        FineScan fs{{count, count}, {part, part}, {out_cs, out_cs}, ncell, nb, &cnt->scan_ticket};
+        k_fine_scan<<<dim3(nb, 1), kScan16Threads, 0, stream>>>(fs);
         KL();
         if (n_max > 0) {
             int grid = std::min(blocks(n_max, 256), 148 * 32);
@@ -619,12 +620,13 @@ template <class R, class RN> class Solver final : public SolverBase {
         const int ncell = LF();
         const int grid = std::min(blocks(std::max(nF, 1), 256), 148 * 32);
         if (nF > 0) {
-            k_bin_key_fluid<R, RN><<<grid, 256, 0, stream>>>(ks, nF, key, rnk, count_f, count_r,
-                                                             part_f, part_r, cnt);
+            k_bin_key_fluid<R, RN><<<grid, 256, 0, stream>>>(ks, nF, key, rnk, count_f, count_r, cnt);
             KL();
         }
         const int nb = (ncell + kScan16Tile - 1) / kScan16Tile;
         FineScan fs{{count_f, count_r}, {part_f, part_r}, {cs, csr}, ncell, nb, &cnt->scan_ticket};
+        k_fine_tile_sums<<<dim3(nb, 2), kScan16Threads, 0, stream>>>(fs);
+        KL();
         k_fine_scan<<<dim3(nb, 2), kScan16Threads, 0, stream>>>(fs);
         KL();
         if (nF > 0) {

@@ -184,15 +184,17 @@ class MPSBatch:
         return inf
 
     def state(self, out: dict | None = None) -> dict:
-        """DevicetoHost: the state in id order, into `out` (e.g. pinned buffers) if given."""
+        """DevicetoHost: the state in id order, into `out` (e.g. pinned buffers) if given;
+        arrays missing from `out` are not copied."""
         n, dt = self.n, self.dtype
         if out is None:
             out = {"typ": np.empty(n, np.int8), "pos": np.empty((3, n), dt),
                    "vel": np.empty((3, n), dt), "acc": np.empty((3, n), dt),
                    "prs": np.empty(n, dt), "pav": np.empty(n, dt)}
-        check(lib().mps_get_state(self._h, out["typ"].ctypes.data_as(L.c_int8_p), _ptr(out["pos"]),
-                                  _ptr(out["vel"]), _ptr(out["acc"]), _ptr(out["prs"]),
-                                  _ptr(out["pav"])), "mps_get_state")
+        t = out.get("typ")
+        check(lib().mps_get_state(self._h, None if t is None else t.ctypes.data_as(L.c_int8_p),
+                                  _ptr(out.get("pos")), _ptr(out.get("vel")), _ptr(out.get("acc")),
+                                  _ptr(out.get("prs")), _ptr(out.get("pav"))), "mps_get_state")
         return out
 
     def set_state(self, typ=None, pos=None, vel=None, acc=None, prs=None, pav=None):

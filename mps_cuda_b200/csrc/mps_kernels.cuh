@@ -885,7 +885,7 @@ __device__ __forceinline__ void gen_reserve_emit(const PassArgs<R, RN>& a, const
 // pass C). Near-wall particles are a thin layer, so this runs as a light kernel of its own
 // instead of stretching the neighbour passes.
 template <class R, class RN, bool DIAG, bool TAPE = false>
-__global__ void __launch_bounds__(128) k_gen_cull(PassArgs<R, RN> a, const V4<R>* gpos,
+__global__ void __launch_bounds__(128, 10) k_gen_cull(PassArgs<R, RN> a, const V4<R>* gpos,
                                                   const R* gprs, const int8_t* gtyp) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     MirrorPlan<R> pl;

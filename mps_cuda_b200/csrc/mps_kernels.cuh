@@ -757,7 +757,7 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
 // reference leaves in d_Acc the velocity ChkCol stored there (kernel.cu:1275, 1620), which
 // UpPcl2 then applies as the acceleration: the velocity after pass B, as here.
 template <class R, class RN, bool DIAG, bool TAPE = false, bool CORR = false>
-__global__ void __launch_bounds__(128, CORR ? 6 : 10) k_pass_c(PassArgs<R, RN> a) {
+__global__ void __launch_bounds__(128, CORR ? 6 : 8) k_pass_c(PassArgs<R, RN> a) {
     using G = typename std::conditional<CORR, GradCorr<R>, GradPlain<R>>::type;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
@@ -786,33 +786,34 @@ __global__ void __launch_bounds__(128, CORR ? 6 : 10) k_pass_c(PassArgs<R, RN> a
         const R rp2 = sc.rp2, rp = sc.rp;
         // P_min over the fluid neighbours inside rp (order-free), then the gradient in order
         R pmin = pi;
-        auto mn = [&](int j, const V4<R>& q) {
+        // each list entry's position and pressure are loaded together (both depend only on
+        // the index), four entries in flight, before the tests that use them
+        auto mn = [&](const V4<R>& q, R pj) {
             R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-            if (dot3(dx, dy, dz, dx, dy, dz) < rp2) {
-                R pj = __ldg(prs + j);
-                if (pj < pmin) pmin = pj;
-            }
+            if (dot3(dx, dy, dz, dx, dy, dz) < rp2 && pj < pmin) pmin = pj;
         };
         int k = 0;
         for (; k + 4 <= n; k += 4) {
             const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
                       j3 = nb[(k + 3) * st];
             V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
-            mn(j0, q0);
-            mn(j1, q1);
-            mn(j2, q2);
-            mn(j3, q3);
+            const R r0 = __ldg(prs + j0), r1 = __ldg(prs + j1), r2 = __ldg(prs + j2),
+                    r3 = __ldg(prs + j3);
+            mn(q0, r0);
+            mn(q1, r1);
+            mn(q2, r2);
+            mn(q3, r3);
         }
         for (; k < n; ++k) {
             const int j = nb[k * st];
-            mn(j, ldg4(pos + j));
+            mn(ldg4(pos + j), __ldg(prs + j));
         }
-        auto gr = [&](int j, const V4<R>& q) {
+        auto gr = [&](const V4<R>& q, R pj) {
             R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
             R d2 = dot3(dx, dy, dz, dx, dy, dz);
             if (d2 < rp2) {
                 R d = sqrtR(d2);
-                g.add(wei_grad(d, rp) / d2, __ldg(prs + j) - pmin, dx, dy, dz);
+                g.add(wei_grad(d, rp) / d2, pj - pmin, dx, dy, dz);
                 ++cf;
             }
         };
@@ -820,14 +821,16 @@ __global__ void __launch_bounds__(128, CORR ? 6 : 10) k_pass_c(PassArgs<R, RN> a
             const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
                       j3 = nb[(k + 3) * st];
             V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
-            gr(j0, q0);
-            gr(j1, q1);
-            gr(j2, q2);
-            gr(j3, q3);
+            const R r0 = __ldg(prs + j0), r1 = __ldg(prs + j1), r2 = __ldg(prs + j2),
+                    r3 = __ldg(prs + j3);
+            gr(q0, r0);
+            gr(q1, r1);
+            gr(q2, r2);
+            gr(q3, r3);
         }
         for (; k < n; ++k) {
             const int j = nb[k * st];
-            gr(j, ldg4(pos + j));
+            gr(ldg4(pos + j), __ldg(prs + j));
         }
         grad_sum_mirrors(sc, c, pid - sc.pbase, p.x, p.y, p.z, pmin, a.m, a.skip != 0, g, cm);
     } else {

@@ -85,12 +85,74 @@ template <class real> class MPS {
     }
     void SetStream(void* cuda_stream) { check(mps_set_stream(h_, cuda_stream), "mps_set_stream"); }
     void SetOption(int opt, int value) { check(mps_set_option(h_, opt, value), "mps_set_option"); }
+    // MPS_GRAD_STANDARD (the compiled PrsGrdTrm) or MPS_GRAD_CORRECTED (its #if 0 variant)
+    void SetGradient(int variant) { SetOption(MPS_OPT_GRADIENT, variant); }
+    // prescribed rigid motion of the OBJ or OBJ2 walls (the declared rotating wall)
+    void SetWallMotion(int type, const double center[3], const double axis[3], double omega,
+                       const double velocity[3]) {
+        check(mps_set_wall_motion(h_, type, center, axis, omega, velocity), "mps_set_wall_motion");
+    }
     mps_handle* handle() { return h_; }
 
    private:
     void phase(int ph) { check(mps_phase(h_, ph), "mps_phase"); }
     mps_handle* h_ = nullptr;
     int n_;
+};
+
+// A case directory as RdDat reads it (MPS_physical.txt + initial.txt, kernel.cu:4-143) and
+// the parameters SetPara derives (kernel.cu:396-415). pos/vel/nrm are SoA with stride n.
+template <class real> struct Case {
+    mps_physical phys;
+    mps_params params;
+    int n = 0;
+    std::vector<int8_t> Typ;
+    std::vector<real> Pos, Vel, Nrm;
+};
+
+template <class real> Case<real> RdDat(const std::string& dir, int precision) {
+    Case<real> c;
+    check(mps_read_physical((dir + "/MPS_physical.txt").c_str(), &c.phys), "mps_read_physical");
+    const std::string init = dir + "/initial.txt";
+    int32_t n = 0;
+    mps_read_initial(init.c_str(), &c.phys, 0, nullptr, nullptr, nullptr, &n);  // sizing call
+    std::vector<double> pos(3 * size_t(n)), nrm(3 * size_t(n));
+    c.Typ.resize(n);
+    check(mps_read_initial(init.c_str(), &c.phys, n, c.Typ.data(), pos.data(), nrm.data(), &n),
+          "mps_read_initial");
+    check(mps_params_from_physical(&c.phys, n, c.Typ.data(), pos.data(), precision, &c.params),
+          "mps_params_from_physical");
+    c.n = n;
+    c.Pos.assign(pos.begin(), pos.end());
+    c.Nrm.assign(nrm.begin(), nrm.end());
+    c.Vel.assign(3 * size_t(n), real(0));
+    return c;
+}
+
+// The reference's output files: WrtDatWLL when constructed, then WrtDat and WrtDat2
+// (kernel.cu:279-304). WrtDat returns once the GPU has copied the state; a writer thread
+// formats the CSV files. Close (or the destructor) waits for them; destroy it before the
+// solver.
+class Output {
+   public:
+    Output(mps_handle* h, const std::string& dir) {
+        check(mps_output_open(h, dir.c_str(), &o_), "mps_output_open");
+    }
+    ~Output() {
+        if (o_) mps_output_close(o_);
+    }
+    Output(const Output&) = delete;
+    Output& operator=(const Output&) = delete;
+    void WrtDat(int iF, double OPT_FQC) { check(mps_output_write(o_, iF, OPT_FQC), "mps_output_write"); }
+    void WrtDat2() { check(mps_output_restart(o_), "mps_output_restart"); }
+    void Close() {
+        const int s = mps_output_close(o_);
+        o_ = nullptr;
+        check(s, "mps_output_close");
+    }
+
+   private:
+    mps_output* o_ = nullptr;
 };
 
 }  // namespace mps_b200

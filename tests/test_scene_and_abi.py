@@ -154,13 +154,16 @@ def test_batched_scene_draws():
 
 
 def test_cpp_facade_compiles_links_and_runs(tmp_path):
-    """include/mps_b200.hpp: a ClcMPS-style loop builds against libmps_b200.so; without a GPU
-    it stops at mps_create with MPS_ERR_NODEVICE, with one it runs 20 steps."""
+    """include/mps_b200.hpp: a ClcMPS-style loop builds against libmps_b200.so. It writes the
+    scene as a case directory and reads it back with RdDat (host only); without a GPU it then
+    stops at mps_create with MPS_ERR_NODEVICE, with one it runs 22 steps and writes the
+    output files."""
     lib = L.library_path()
     exe = tmp_path / "clcmps_loop"
     src = os.path.join(ROOT, "tests", "cpp", "clcmps_loop.cpp")
     subprocess.run(["/usr/bin/g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), src,
                     "-L", os.path.dirname(lib), "-lmps_b200", "-Wl,-rpath," + os.path.dirname(lib),
                     "-o", str(exe)], check=True, capture_output=True)
-    res = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    res = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=300)
     assert res.returncode == 0, res.stdout + res.stderr
+    assert "case: " in res.stdout

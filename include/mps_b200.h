@@ -151,7 +151,12 @@ enum {
     MPS_OPT_CELL_SKIP = 3,   /* 1: skip bucket rows outside the radius (default 1)      */
     MPS_OPT_TIMING = 4,      /* 1: time every kernel group of mps_step with CUDA events
                                 on the handle's stream (steps then run without a graph) */
-    MPS_OPT_GRADIENT = 5     /* PrsGrdTrm variant, MPS_GRAD_* (default STANDARD)        */
+    MPS_OPT_GRADIENT = 5,    /* PrsGrdTrm variant, MPS_GRAD_* (default STANDARD)        */
+    MPS_OPT_LIST_CAPACITY = 6 /* neighbour-list entries kept per particle between ChkCol/
+                                MkPrs and PrsGrdTrm: 0 or above 160 = 160 (the default).
+                                A particle with more neighbours walks its fine cells again
+                                instead, with the same result; lower values exercise that
+                                path. Changing it voids a recorded adjoint rollout.       */
 };
 
 /* PrsGrdTrm variants (MPS_OPT_GRADIENT). STANDARD is the kernel the reference compiles

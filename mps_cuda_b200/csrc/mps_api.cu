@@ -157,6 +157,10 @@ int mps_set_option(mps_handle* h, int32_t opt, int32_t value) {
                 break;
             case MPS_OPT_CELL_SKIP: s.skip_opt = value != 0; s.invalidate_graph(); break;
             case MPS_OPT_TIMING: s.timing_on = value != 0; break;
+            case MPS_OPT_LIST_CAPACITY:
+                if (value < 0) throw ApiError(MPS_ERR_ARG, "list capacity must not be negative");
+                s.set_list_capacity(value);
+                break;
             case MPS_OPT_GRADIENT:
                 if (value != MPS_GRAD_STANDARD && value != MPS_GRAD_CORRECTED)
                     throw ApiError(MPS_ERR_ARG, "gradient must be MPS_GRAD_STANDARD or _CORRECTED");

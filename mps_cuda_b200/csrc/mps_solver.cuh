@@ -267,6 +267,7 @@ struct SolverBase {
     virtual void get_counters(mps_counters*) = 0;
     virtual void integrals(int scene, double out[6]) = 0;
     virtual void invalidate_graph() = 0;
+    virtual void set_list_capacity(int k) = 0;  // 0: the full capacity
     // WrtDat's snapshot into device staging (id order, state type) and the second mirror
     // generation; the mirror count goes to pinned host memory. Then pav = 0 (kernel.cu:289).
     virtual void output_snapshot(void* pos, void* vel, void* prs, void* pav, int8_t* typ,
@@ -329,7 +330,8 @@ template <class R, class RN> class Solver final : public SolverBase {
     int* nb;
     int* nbcnt;
     int8_t* near_wall;
-    int nbK = 160;  // list capacity: about 125 neighbours lie inside r at rest density
+    static constexpr int kListCap = 160;  // about 125 neighbours lie inside r at rest density
+    int nbK = kListCap;                    // list capacity in use (MPS_OPT_LIST_CAPACITY)
     std::vector<int> fluid_ids, wall_ids;
     bool lists_valid = false, sorted = false, m1_valid = false, acc_dirty = false;
     cudaGraphExec_t gexec = nullptr;
@@ -573,7 +575,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         io.typ = ar.template get<int8_t>(T);
         io.cell = ar.template get<int>(T);
         d_integ = ar.template get<double>(6 * size_t(nscene));
-        nb = ar.template get<int>(size_t(nbK) * F);
+        nb = ar.template get<int>(size_t(kListCap) * F);
         near_wall = ar.template get<int8_t>(L());
         nbcnt = ar.template get<int>(F);
         CK(cudaMemsetAsync(S.acc, 0, sizeof(V4<R>) * F, stream));
@@ -841,6 +843,11 @@ template <class R, class RN> class Solver final : public SolverBase {
         CK(cudaStreamSynchronize(stream));
         if (chosen)
             for (int k = 0; k < MPS_K_COUNT; ++k) chosen[k] = blk[k];
+    }
+
+    void set_list_capacity(int k) override {
+        nbK = (k == 0 || k > kListCap) ? kListCap : k;
+        invalidate_graph();  // the captured launches carry the capacity
     }
 
     void invalidate_graph() override {
@@ -1160,6 +1167,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     struct AdjState {
         DevArena ar;
         int nsteps = 0, every = 0, nck = 0;
+        int nbK = 0;  // list capacity the tape was allocated and recorded with
         long long steps_end = 0;
         std::vector<Ckpt> ck;  // nck segment starts + the final state
         std::vector<TapeStep<R>> tape;
@@ -1194,6 +1202,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     void adj_alloc(int nck, int every) {
         adj.reset();
         auto st = std::make_unique<AdjState>();
+        st->nbK = nbK;
         DevArena& a = st->ar;
         const size_t F = std::max(nF, 1), T = std::max(nT, 1), Cm = size_t(cap), Lc = L() + 1;
         for (int c = 0; c <= nck; ++c)
@@ -1358,6 +1367,9 @@ template <class R, class RN> class Solver final : public SolverBase {
                           double* g_vel, double* g_nu) override {
         if (!adj || adj->nsteps == 0)
             throw ApiError(MPS_ERR_STATE, "no recorded rollout: call mps_adjoint_record first");
+        if (adj->nbK != nbK)
+            throw ApiError(MPS_ERR_STATE, "the neighbour-list capacity changed since the rollout "
+                                          "was recorded");
         if (nF == 0) return;
         AdjState& s = *adj;
         const size_t T = size_t(nT);

@@ -204,3 +204,44 @@ def test_batch_of_64_uneven_scenes_equals_separate_handles():
         _assert_same_state(sub, h.state())
         h.close()
         off += n
+
+
+@pytest.mark.parametrize("prec", [F32, F64])
+@pytest.mark.parametrize("cap", [1, 8])
+def test_list_overflow_path_bit_exact(prec, cap):
+    """A particle whose neighbour list would exceed its capacity walks its fine cells again in
+    ChkCol/MkPrs and PrsGrdTrm. MPS_OPT_LIST_CAPACITY forces that path on for (nearly) every
+    particle: the state, the mirrors and the neighbour counts stay those of the oracle."""
+    g, o, _, _ = _pair("dambreak_l0.02_small", prec)
+    g.set_option(L.OPT_LIST_CAPACITY, cap)
+    g.set_option(L.OPT_GRAPH, 1)
+    try:
+        for chunk in (1, 4, 15):
+            g.step(chunk)
+            o.step(chunk)
+            _assert_same_state(g.state(), o.state(), (cap, chunk))
+        dg, do = g.diag(), o.diag()
+        fl = o.state()["typ"] == 0
+        for c in ("col_f", "col_w", "col_m", "prs_f", "prs_m", "grd_f", "grd_m"):
+            assert np.array_equal(dg[c][fl], do[c][fl]), c
+        _assert_same_mirrors(g.mirrors(2), o.mirrors())
+        g.set_option(L.OPT_LIST_CAPACITY, 0)  # back to the full lists
+        g.step(3)
+        o.step(3)
+        _assert_same_state(g.state(), o.state(), (cap, "full"))
+    finally:
+        g.close()
+
+
+def test_list_capacity_change_voids_a_recorded_rollout():
+    g, _, _, _ = _pair("dambreak_l0.02_small", F64, diag=False)
+    try:
+        g.adjoint_record(4, 2)
+        g.set_option(L.OPT_LIST_CAPACITY, 8)
+        with pytest.raises(MPSError) as e:
+            g.adjoint_backward(np.zeros((3, g.n)), np.zeros((3, g.n)))
+        assert e.value.code == L.MPS_ERR_STATE
+        with pytest.raises(MPSError):
+            g.set_option(L.OPT_LIST_CAPACITY, -1)
+    finally:
+        g.close()

@@ -139,3 +139,34 @@ def test_adjoint_refuses_the_corrected_gradient():
         assert e.value.code == L.MPS_ERR_UNSUPPORTED
     finally:
         g.close()
+
+
+def test_batched_scenes_with_the_corrected_gradient():
+    """Two scenes in one handle, corrected gradient on: each equals its own oracle."""
+    from mps_cuda_b200 import MPSBatch
+    descs = []
+    for k in range(2):
+        d, dt, _ = configs.WORKLOADS["dambreak_l0.02_small"]
+        descs.append((type(d)(**{**d.__dict__, "seed": d.seed + 7 * k}), dt))
+    parts = [dambreak(d) for d, _ in descs]
+    params = [dambreak_params(d, dt=dt, precision=F64) for d, dt in descs]
+    cat = lambda key: np.concatenate([p[key] for p in parts], axis=-1)
+    counts = [p["typ"].shape[0] for p in parts]
+    b = MPSBatch(params, cat("typ"), cat("pos"), cat("vel"), cat("nrm"), counts=counts)
+    b.set_option(L.OPT_GRADIENT, L.GRAD_CORRECTED)
+    ors = []
+    for pp, pt in zip(params, parts):
+        o = Oracle(params_from(pp), pt["typ"], pt["pos"], pt["vel"], pt["nrm"])
+        o.set_gradient(1)
+        ors.append(o)
+    try:
+        b.step(8)
+        for o in ors:
+            o.step(8)
+        st = b.state()
+        off = 0
+        for s, (o, n) in enumerate(zip(ors, counts)):
+            _same({k: v[..., off:off + n] for k, v in st.items()}, o.state(), s)
+            off += n
+    finally:
+        b.close()

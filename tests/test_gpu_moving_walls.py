@@ -157,3 +157,16 @@ def test_errors():
         assert e.value.code == L.MPS_ERR_UNSUPPORTED
     finally:
         g.close()
+
+
+def test_moving_plate_with_the_corrected_gradient():
+    """The two options together: still the oracle's state, exactly."""
+    g, o, _, _ = _pair(F64)
+    g.set_option(L.OPT_GRADIENT, L.GRAD_CORRECTED)
+    o.set_gradient(1)
+    try:
+        g.step(12)
+        o.step(12)
+        _same(g.state(), o.state(), "corrected + moving")
+    finally:
+        g.close()

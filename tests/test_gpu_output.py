@@ -151,3 +151,26 @@ def test_run_case_end_to_end(tmp_path):
     z0 = np.loadtxt(out / "output00000.csv", delimiter=",", skiprows=1)[:, 2].mean()
     z1 = np.loadtxt(out / f"output{res['files'] - 1:05d}.csv", delimiter=",", skiprows=1)[:, 2].mean()
     assert z1 < z0
+
+
+def test_output_of_a_two_scene_handle(tmp_path):
+    """A batched handle writes the fluid of every scene, scene after scene in id order."""
+    from mps_cuda_b200 import MPSBatch
+    select_device(0)
+    parts = [dambreak(DESC), dambreak(SceneDesc(l0=0.02, tank=(0.4, 0.2, 0.4), block=(6, 6, 6),
+                                                 jitter=0.01, seed=9))]
+    cat = lambda key: np.concatenate([p[key] for p in parts], axis=-1)
+    counts = [p["typ"].shape[0] for p in parts]
+    params = [dambreak_params(DESC, dt=2e-4, precision=F32)] * 2
+    b = MPSBatch(params, cat("typ"), cat("pos").astype(np.float32), cat("vel").astype(np.float32),
+                 cat("nrm").astype(np.float32), counts=counts)
+    try:
+        with files.Output(b, str(tmp_path)) as out:
+            b.step(6)
+            st = b.state()
+            out.write(1, 6.0)
+        lines = _lines(tmp_path / "output00001.csv")
+        assert lines[1:] == _fluid_rows(st, 6.0, F32)
+        assert len(lines) - 1 == int((st["typ"] == L.FLD).sum()) == 480 + 216
+    finally:
+        b.close()

@@ -89,3 +89,22 @@ def test_missing_rank_ends_with_an_error():
         p.kill()
         pytest.fail("the rendezvous of a missing rank did not time out")
     assert q.get(timeout=5) != "joined"
+
+
+def test_reference_arm_under_two_ranks():
+    """`bench.py --impl reference` launched as two ranks: rank 0 times the CPU restatement and
+    prints the one JSON line, rank 1 does no work, and both exit 0."""
+    import json
+    import subprocess
+    env = dict(os.environ, MPS_BENCH_BACKEND="gloo")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),
+           os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+           "--workload", "dambreak_l0.02_small", "--steps", "2", "--warmup", "1"]
+    res = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stdout[-2000:] + res.stderr[-2000:]
+    lines = [l for l in res.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, res.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["n_gpus"] == 2
+    assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0

@@ -82,3 +82,23 @@ def test_skipping_bucket_rows_changes_nothing(big):
     a.step(2)
     b.step(2)
     _same(a.state(), b.state())
+
+
+def test_full_size_steps_equal_the_oracle(big):
+    """At the benchmark's own size (384 000 fluid particles, FP32) two fused steps give the
+    oracle's state exactly, mirrors included."""
+    from oracle.oracle import Oracle, params_from
+    p, args = big
+    g = MPS(p, *args)
+    o = Oracle(params_from(p), *args)
+    try:
+        g.step(2)
+        o.step(2)
+        a, b = g.state(), o.state()
+        for k in ("typ", "pos", "vel", "prs", "pav"):
+            assert np.array_equal(a[k], b[k]), k
+        gm, om = g.mirrors(2), o.mirrors()
+        assert len(gm["slot"]) > 80000
+        assert np.array_equal(gm["slot"], om["slot"]) and np.array_equal(gm["pos"], om["pos"])
+    finally:
+        g.close()

@@ -3,9 +3,10 @@
 
 A step is one pass of the dam-break time step (frsykzk/MPS_CUDA kernel.cu:1904-1941) over
 all fluid particles of the workload; a particle-update is one fluid particle advanced
-through one step. The default workload is the 384 000-particle dam break (l0 = 0.005 m,
-0.4 x 0.2 x 0.6 m column in a 1.6 x 0.2 x 0.8 m tank, dt = 5e-5 s), FP32, on synthetic
-seeded inputs (there is no dataset).
+through one step. The default workload is the largest single-GPU scene: 6 144 000 fluid and
+614 400 wall particles (l0 = 0.0025 m, 0.4 x 0.4 x 0.6 m column in a 1.6 x 0.4 x 0.8 m tank,
+dt = 2.5e-5 s, bucket rebuild every step), FP32 (the reference's `typedef float real`), on
+synthetic seeded inputs (there is no dataset).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -19,11 +20,13 @@ ours      : libmps_b200.so. `value` = device time of K steps (CUDA events on the
             `batched` = 64 uneven scenes in one handle against a per-scene loop;
             `adjoint` = the rollout adjoint's cost per step against a forward step at the
             48 000-particle adjoint workload, with its finite-difference agreement;
-            `other_workloads` = the same workload in FP64 and the 6.1M-particle scene.
+            `other_workloads` = the 384 000-particle dam break in FP32 and FP64.
 reference : the reference's per-particle loops as that OpenMP CPU restatement (the
-            reference itself has no CPU implementation), all host threads, rank 0 only;
-            `reference_cuda` adds the reference's own CUDA kernels (built for sm_100a from
-            its sources) on the same workload and GPU, where that build is present.
+            reference itself has no CPU implementation), all host threads, rank 0 only, on
+            the same workload built by the oracle's own scene generator (the product library
+            is not loaded); `reference_cuda` adds the reference's own CUDA kernels (built for
+            sm_100a from its sources) on the same workload and GPU, where that build is
+            present.
 Under torchrun (N > 1) each rank advances its own copy of the workload on its own GPU
 (replicas: the step has no exchange between scenes), so `value` counts all ranks' updates.
 """
@@ -44,7 +47,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle-updates/s"
-WORKLOAD = "dambreak_l0.005_384k"
+WORKLOAD = "dambreak_l0.0025_6.1M"
 L2_FLUSH_BYTES = 512 << 20  # > 126 MB L2
 
 # Algorithmic bytes per unit (s = sizeof(real)): the state each kernel group must move,
@@ -179,22 +182,48 @@ def build_scene(workload: str, precision: str):
     return p, sc["typ"], sc["pos"].astype(rd), sc["vel"].astype(rd), sc["nrm"].astype(rd)
 
 
+def build_scene_oracle(workload: str, precision: str):
+    """The same workload from the oracle's own scene generator (tests/test_oracle_scene.py
+    checks it byte for byte against build_scene), for the reference arm, which must not load
+    the product library."""
+    from oracle import scenes
+    return scenes.workload(workload, precision)
+
+
+def bench_config(workload: str, precision: str, nf: int, nw: int, world: int) -> dict:
+    """The `config` object of both arms' JSON lines."""
+    return {"workload": workload, "fluid_particles": nf, "wall_particles": nw,
+            "precision": precision,
+            "scene": "synthetic seeded dam break (walls on five tank faces, jittered lattice)",
+            "l2": "state larger than the 126 MB L2; the GPU arm also flushes L2 (512 MiB "
+                  "write) between timed steps",
+            "parallelism": f"replicas x{world}"}
+
+
 def cpu_oracle_rate(p, typ, pos, vel, nrm, budget_s: float, max_steps: int, warmup: int = 1):
-    """Particle-updates/s of the OpenMP oracle; returns (rate, steps timed, threads)."""
+    """Particle-updates/s of the OpenMP oracle over whole steps of the workload.
+
+    `warmup` untimed steps, then at most `max_steps` timed steps, fewer where the warm-up
+    steps' pace says they would take longer than `budget_s`. Returns (rate, steps timed,
+    threads, seconds, warm-up steps run)."""
     from oracle.oracle import Oracle, lib, params_from
     threads = os.cpu_count() or 1
     lib().oracle_set_threads(threads)
     o = Oracle(params_from(p), typ, pos, vel, nrm)
     nf = int((typ == 0).sum())
+    w = max(warmup, 1)
     t0 = time.perf_counter()
-    o.step(max(warmup, 1))
-    t_step = (time.perf_counter() - t0) / max(warmup, 1)
+    o.step(1)
+    t_step = time.perf_counter() - t0
+    if w > 1:  # the remaining warm-up steps, as far as the budget allows
+        w = 1 + int(min(w - 1, max(0.0, budget_s / 4) // max(t_step, 1e-9)))
+        o.step(w - 1)
     k = int(max(1, min(max_steps, budget_s // max(t_step, 1e-9))))
     t0 = time.perf_counter()
     o.step(k)
     el = time.perf_counter() - t0
     o.close()
-    return nf * k / el, k, threads, el
+    return nf * k / el, k, threads, el, w
 
 
 @contextlib.contextmanager
@@ -224,11 +253,10 @@ def reference_cuda_rate(p, typ, pos, vel, nrm, steps: int, warmup: int):
     wall clock around that synchronised loop, L2 not flushed. None where the library or a GPU
     is missing, or for the mixed precision the reference does not have.
     """
-    from mps_cuda_b200 import F32, F64
-    if p.precision not in (F32, F64):
+    if p.precision not in (0, 1):  # float or double: the reference has no mixed precision
         return None
     from oracle import refbind
-    prec = 1 if p.precision == F64 else 0
+    prec = p.precision
     if not refbind.available(prec):
         return None
     import torch
@@ -251,20 +279,22 @@ def reference_cuda_rate(p, typ, pos, vel, nrm, steps: int, warmup: int):
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    p, typ, pos, vel, nrm = build_scene(args.workload, args.precision)
-    rate, k, threads, el = cpu_oracle_rate(p, typ, pos, vel, nrm, budget_s=150.0,
-                                           max_steps=args.steps, warmup=min(args.warmup, 2))
+    p, typ, pos, vel, nrm = build_scene_oracle(args.workload, args.precision)
+    nf, nw = int((typ == 0).sum()), int((typ != 0).sum())
+    rate, k, threads, el, w = cpu_oracle_rate(p, typ, pos, vel, nrm, budget_s=150.0,
+                                              max_steps=args.steps, warmup=args.warmup)
     ref_cuda = reference_cuda_rate(p, typ, pos, vel, nrm, steps=args.steps,
                                    warmup=max(args.warmup, 3))
-    sample = (f"{k} full steps of the {args.workload} workload ({int((typ == 0).sum())} fluid "
-              f"particles) after {min(args.warmup, 2)} warm-up step(s), {threads} OpenMP threads")
+    sample = (f"{k} whole steps of the {args.workload} workload ({nf} fluid particles) after "
+              f"{w} warm-up step(s), {threads} OpenMP threads")
     line = {"metric": METRIC, "value": rate, "unit": "particle-updates/s", "impl": "reference",
-            "n_gpus": args.gpus, "steps": k, "warmup": min(args.warmup, 2),
+            "n_gpus": args.gpus, "steps": k, "warmup": w,
             "ms_per_step": 1e3 * el / k, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
-            "config": {"workload": args.workload, "precision": args.precision,
-                       "implementation": "OpenMP CPU restatement of the reference's per-particle "
-                                         "loops (the reference has no CPU path)"},
+            "config": bench_config(args.workload, args.precision, nf, nw, world),
+            "implementation": "OpenMP CPU restatement of the reference's per-particle loops "
+                              "(the reference has no CPU path), scene from the oracle's own "
+                              "generator",
             "cpu_baseline": {"value": rate, "unit": "particle-updates/s", "cores": threads,
                              "kind": "port", "sample": sample},
             "e2e": {"value": rate, "unit": "particle-updates/s", "h2d_bytes_per_step": 0,
@@ -387,15 +417,18 @@ def run_ours(args, world, rank, local):
         adjoint = measure_adjoint(stream)
     extra = None
     if not args.no_extra:
-        # the same workload in FP64, and the 6.1M-particle single scene in FP32
-        extra = [measure_workload(args.workload, "f64", stream, flush, min(K, 50)),
-                 measure_workload("dambreak_l0.0025_6.1M", "f32", stream, flush, min(K, 20))]
+        # the 384 000-particle dam break in FP32 and FP64 (the reference dtype of its config)
+        extra = [measure_workload(w_, pr_, stream, flush, min(K, 50))
+                 for w_, pr_ in (("dambreak_l0.005_384k", "f32"), ("dambreak_l0.005_384k", "f64"))
+                 if (w_, pr_) != (args.workload, args.precision)]
     clk.__exit__(None, None, None)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, k, threads, el = cpu_oracle_rate(p, typ, pos, vel, nrm, budget_s=20.0, max_steps=200)
+        rate, k, threads, el, w = cpu_oracle_rate(p, typ, pos, vel, nrm, budget_s=20.0,
+                                                  max_steps=200)
         cpu = {"value": rate, "unit": "particle-updates/s", "cores": threads, "kind": "port",
-               "sample": f"{k} steps of the same workload after 1 warm-up step ({el:.1f} s)"}
+               "sample": f"{k} whole steps of the same workload after {w} warm-up step(s) "
+                         f"({el:.1f} s)"}
 
     if rank == 0:
         line = {
@@ -403,10 +436,9 @@ def run_ours(args, world, rank, local):
             "steps": K, "warmup": max(args.warmup, 3), "ms_per_step": dev_ms_max / K,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": args.precision, "data": "synthetic",
-            "config": {"workload": args.workload, "fluid_particles": nf,
-                       "wall_particles": int((typ != 0).sum()), "precision": args.precision,
-                       "l2": "flushed between timed steps (512 MiB write)",
-                       "parallelism": f"replicas x{world}", "graph": True},
+            "config": bench_config(args.workload, args.precision, nf, int((typ != 0).sum()),
+                                   world),
+            "graph": True,
             "clocks": clk.summary(), "wall_ms_per_step": 1e3 * wall / K,
             "e2e": e2e, "gpu_launches": launches,
             "roofline": roofline, "kernel_groups": groups, "cpu_baseline": cpu,

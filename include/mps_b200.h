@@ -431,7 +431,10 @@ int mps_output_close(mps_output* o);
  * or MPS_NOALLOC_MAX_BUCKETS buckets are rejected with MPS_ERR_OVERFLOW. All calls on a
  * device share the array: calls whose work overlaps on the GPU race, so serialise them on
  * one stream. The first call on a device looks up the array's address there; make it
- * before any stream capture.
+ * before any stream capture. That address is kept for the life of the process, so do not
+ * call this entry point on a device after a cudaDeviceReset of it. A particle outside the
+ * bucket grid gets the nearest edge bucket (its coordinates are clamped, as the solver
+ * does) and nothing reports it: check positions first where particles may leave the domain.
  */
 int mps_bucket_build_noalloc(const mps_params* p, int32_t n, const int8_t* typ, const void* pos,
                              int32_t* cell, int32_t* order, int32_t* start, void* stream);

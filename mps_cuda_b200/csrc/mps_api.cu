@@ -45,6 +45,28 @@ int check_params(const mps_params& p) {
     if (p.precision < 0 || p.precision > 2) return fail(MPS_ERR_ARG, "unknown precision");
     return MPS_OK;
 }
+
+// derived constants of a scene in its precision (host only); a grid too large for the
+// int32 cell indices is reported here, before any device is touched
+int derive_checked(const mps_params& p, mps_info* out) {
+    mps_info tmp;
+    if (!out) out = &tmp;
+    try {
+        if (p.precision == 1) {
+            mps::SceneDev<double, double> sd;
+            mps::derive_scene<double, double>(p, 0, 0, 0, 0, sd, *out);
+        } else if (p.precision == 2) {
+            mps::SceneDev<float, double> sd;
+            mps::derive_scene<float, double>(p, 0, 0, 0, 0, sd, *out);
+        } else {
+            mps::SceneDev<float, float> sd;
+            mps::derive_scene<float, float>(p, 0, 0, 0, 0, sd, *out);
+        }
+    } catch (const ApiError& e) {
+        return fail(e.code, e.what());
+    }
+    return MPS_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -59,6 +81,7 @@ int mps_create_batch(int32_t nscenes, const mps_params* p, const int32_t* counts
     long long total = 0;
     for (int s = 0; s < nscenes; ++s) {
         int rc = check_params(p[s]);
+        if (!rc) rc = derive_checked(p[s], nullptr);
         if (rc) return rc;
         if (p[s].precision != p[0].precision)
             return fail(MPS_ERR_ARG, "every scene of a batch must use the same precision");
@@ -106,17 +129,7 @@ int mps_derive(const mps_params* p, mps_info* out) {
     if (!p || !out) return fail(MPS_ERR_ARG, "null argument");
     int rc = check_params(*p);
     if (rc) return rc;
-    if (p->precision == 1) {
-        mps::SceneDev<double, double> sd;
-        mps::derive_scene<double, double>(*p, 0, 0, 0, 0, sd, *out);
-    } else if (p->precision == 2) {
-        mps::SceneDev<float, double> sd;
-        mps::derive_scene<float, double>(*p, 0, 0, 0, 0, sd, *out);
-    } else {
-        mps::SceneDev<float, float> sd;
-        mps::derive_scene<float, float>(*p, 0, 0, 0, 0, sd, *out);
-    }
-    return MPS_OK;
+    return derive_checked(*p, out);
 }
 
 int mps_create(const mps_params* p, int32_t n, const int8_t* typ, const void* pos,

@@ -17,7 +17,15 @@
 //   * the array keeps the previous call's contents; each call clears the counters it
 //     needs before using them;
 //   * the first call on a device looks up the array's device address there
-//     (cudaGetSymbolAddress); make that first call before any stream capture.
+//     (cudaGetSymbolAddress); make that first call before any stream capture. The address
+//     is kept per device ordinal for the life of the process: after a cudaDeviceReset the
+//     library's module is loaded again in the new context and the kept address no longer
+//     names the array, so a process that resets a device must not call this entry point
+//     on that device afterwards;
+//   * like the reference's cell index (kernel.cu:521-524), a particle outside the bucket
+//     grid gets the nearest edge bucket: cell_of clamps its coordinates. Nothing reports
+//     that here (the solver counts such particles in err_cell_range); a caller whose
+//     particles may leave the domain checks their positions itself.
 #include <mutex>
 
 #include "mps_solver.cuh"
@@ -36,17 +44,24 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 int* g_addr[kMaxDevices] = {};
 
-// host-side address of g_scratch on the current device
-int scratch_on_current_device(int* dev_out, int** out) {
+// host-side address of g_scratch on the current device; a failing CUDA call's error is
+// returned in *err (it is consumed here and cannot be read again with cudaGetLastError)
+int scratch_on_current_device(int* dev_out, int** out, cudaError_t* err) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return MPS_ERR_CUDA;
+    if (e != cudaSuccess) {
+        *err = e;
+        return MPS_ERR_CUDA;
+    }
     if (dev < 0 || dev >= kMaxDevices) return MPS_ERR_UNSUPPORTED;
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_addr[dev]) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_scratch);
-        if (e != cudaSuccess || !p) return MPS_ERR_CUDA;
+        if (e != cudaSuccess || !p) {
+            *err = e != cudaSuccess ? e : cudaErrorInvalidSymbol;
+            return MPS_ERR_CUDA;
+        }
         g_addr[dev] = static_cast<int*>(p);
     }
     *dev_out = dev;
@@ -91,14 +106,18 @@ __global__ void k_copy_starts(const int* cs, int nb, int* start) {
 
 template <class R>
 int run(const mps_params& p, int n, const int8_t* typ, const void* pos, int32_t* cell,
-        int32_t* order, int32_t* start, cudaStream_t st) {
+        int32_t* order, int32_t* start, cudaStream_t st, cudaError_t* err) {
     SceneDev<R, R> sc;
     mps_info inf;
-    derive_scene<R, R>(p, 0, 0, 0, n, sc, inf);
+    try {
+        derive_scene<R, R>(p, 0, 0, 0, n, sc, inf);  // host only: checks the grid's size
+    } catch (const ApiError& e) {
+        return e.code;
+    }
     const int C = inf.nbxyz;
     if (C > MPS_NOALLOC_MAX_BUCKETS) return MPS_ERR_OVERFLOW;
     int dev = 0, *base = nullptr;
-    int rc = scratch_on_current_device(&dev, &base);
+    int rc = scratch_on_current_device(&dev, &base, err);
     if (rc) return rc;
     const int L = C + 1;  // buckets + the bucket of GST particles
     int* key = base;
@@ -123,8 +142,8 @@ int run(const mps_params& p, int n, const int8_t* typ, const void* pos, int32_t*
                                                                   seg, C);
     }
     k_copy_starts<<<gc, 256, 0, st>>>(cs, C, start);
-    cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? MPS_OK : MPS_ERR_CUDA;
+    *err = cudaGetLastError();
+    return *err == cudaSuccess ? MPS_OK : MPS_ERR_CUDA;
 }
 
 }  // namespace
@@ -137,6 +156,9 @@ extern "C" int mps_bucket_build_noalloc(const mps_params* p, int32_t n, const in
         mps::g_last_error = "mps_bucket_build_noalloc: null argument or negative count";
         return MPS_ERR_ARG;
     }
+    // The size checks stay ahead of every device access: a caller may pass buffers that
+    // were sized for the limit, and a size beyond it must fail before any kernel or copy
+    // touches them.
     if (n > MPS_NOALLOC_MAX_ITEMS) {
         mps::g_last_error = "mps_bucket_build_noalloc: more than MPS_NOALLOC_MAX_ITEMS particles";
         return MPS_ERR_OVERFLOW;
@@ -148,15 +170,15 @@ extern "C" int mps_bucket_build_noalloc(const mps_params* p, int32_t n, const in
         return MPS_ERR_ARG;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t err = cudaSuccess;
     int rc = p->precision == MPS_F64
-                 ? mps::run<double>(*p, n, typ, pos, cell, order, start, st)
-                 : mps::run<float>(*p, n, typ, pos, cell, order, start, st);
+                 ? mps::run<double>(*p, n, typ, pos, cell, order, start, st, &err)
+                 : mps::run<float>(*p, n, typ, pos, cell, order, start, st, &err);
     if (rc == MPS_ERR_OVERFLOW)
         mps::g_last_error = "mps_bucket_build_noalloc: the grid has more than "
                             "MPS_NOALLOC_MAX_BUCKETS buckets";
     else if (rc == MPS_ERR_CUDA)
-        mps::g_last_error = std::string("mps_bucket_build_noalloc: ") +
-                            cudaGetErrorString(cudaGetLastError());
+        mps::g_last_error = std::string("mps_bucket_build_noalloc: ") + cudaGetErrorString(err);
     else if (rc == MPS_ERR_UNSUPPORTED)
         mps::g_last_error = "mps_bucket_build_noalloc: device ordinal beyond 63";
     return rc;

@@ -48,6 +48,11 @@ struct ApiError : std::runtime_error {
     } while (0)
 
 // ---- derived constants (AlcBkt + SetPara, kernel.cu:307-415) ----------------------------
+// Grid limits: fine cells (27 per bucket, plus the cell of unlisted particles and the end
+// of the start table) are indexed by int32 across all scenes of a handle.
+constexpr long long kMaxBucketsPerAxis = 1LL << 20;
+constexpr long long kMaxFineCells = (1LL << 31) - 2;
+
 template <class R> static R wei(R d, R re) { return ((re / d) + (d / re)) - R(2); }
 template <class R> static R wei_grad_h(R d, R re) { return (re / d) - (d / re); }
 
@@ -80,9 +85,25 @@ static void derive_scene(const mps_params& p, int cbase, int fbase, int pbase, i
     const R db = l0 * R(3.1), dbinv = R(1) / db;
     s.db = db;
     s.dbinv = dbinv;
-    s.nbx = int((maxc[0] - s.minc[0]) * dbinv) + 3;  // kernel.cu:317-319
-    s.nby = int((maxc[1] - s.minc[1]) * dbinv) + 3;
-    s.nbz = int((maxc[2] - s.minc[2]) * dbinv) + 3;
+    // kernel.cu:317-319. The extents are checked before any int conversion, and the bucket
+    // count in 64 bits, so that no grid too large for the int32 cell indices of the bucket
+    // builds (27 fine cells per bucket, plus the unlisted cell) wraps to a small value.
+    long long nbl[3];
+    for (int d = 0; d < 3; ++d) {
+        const R t = (maxc[d] - s.minc[d]) * dbinv;
+        if (!(t >= R(0) && t < R(kMaxBucketsPerAxis)))
+            throw ApiError(MPS_ERR_OVERFLOW, "the bucket grid has more than " +
+                                                 std::to_string(kMaxBucketsPerAxis) +
+                                                 " buckets along an axis");
+        nbl[d] = (long long)(t) + 3;
+    }
+    const long long nbxyz = nbl[0] * nbl[1] * nbl[2];
+    if (27 * nbxyz + 2 > kMaxFineCells)
+        throw ApiError(MPS_ERR_OVERFLOW, "the bucket grid needs " + std::to_string(nbxyz) +
+                                             " buckets, more than int32 fine-cell indices hold");
+    s.nbx = int(nbl[0]);
+    s.nby = int(nbl[1]);
+    s.nbz = int(nbl[2]);
     s.nbxy = s.nbx * s.nby;
     s.cbase = cbase;
     s.pbase = pbase;
@@ -426,18 +447,23 @@ template <class R, class RN> class Solver final : public SolverBase {
         for (int s = 0; s < ns; ++s) nT += cnts[s];
         hsc.resize(ns);
         infos.resize(ns);
-        int cb = 0, pb = 0;
-        long long fb = 0;
+        long long cb = 0, fb = 0;
+        int pb = 0;
         for (int s = 0; s < ns; ++s) {
-            derive_scene<R, RN>(p[s], cb, int(fb), pb, cnts[s], hsc[s], infos[s]);
+            // each scene's grid fits (derive_scene checks it); the sum over scenes is checked
+            // before its base offsets are used
+            if (fb + 27LL + 2 > kMaxFineCells)
+                throw ApiError(MPS_ERR_OVERFLOW, "the scenes' fine cell grids need more cells "
+                                                 "than an int32 index holds");
+            derive_scene<R, RN>(p[s], int(cb), int(fb), pb, cnts[s], hsc[s], infos[s]);
             cb += infos[s].nbxyz;
             fb += 27LL * infos[s].nbxyz;
             pb += cnts[s];
+            if (fb + 2 > kMaxFineCells)
+                throw ApiError(MPS_ERR_OVERFLOW, "the fine cell grid needs " + std::to_string(fb) +
+                                                     " cells, more than an int32 index holds");
         }
-        if (fb >= (1LL << 31) - 2)
-            throw ApiError(MPS_ERR_OVERFLOW, "the fine cell grid needs " + std::to_string(fb) +
-                                                 " cells, more than an int32 index holds");
-        C = cb;
+        C = int(cb);
         CF = int(fb);
         // classify particles: walls inside the padded box are static walls, everything
         // else is a fluid-class particle; RdDat drops what lies outside (kernel.cu:117)

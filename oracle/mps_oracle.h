@@ -25,6 +25,25 @@ typedef struct oracle_params {
     int32_t reserved[7];
 } oracle_params;
 
+/* Dam-break scene description (same field order as mps_scene_desc): oracle_scene.cpp */
+typedef struct oracle_scene_desc {
+    double l0, tank[3];
+    int32_t block[3], wall_mask;
+    double jitter;
+    uint64_t seed;
+    double vel_sigma;
+    uint64_t vel_seed;
+    double origin[3];
+} oracle_scene_desc;
+
+/* particles of a dam-break scene; typ[n], pos/vel/nrm double SoA with stride cap */
+int oracle_scene_dambreak_count(const oracle_scene_desc* d, int32_t* n_out);
+int oracle_scene_dambreak(const oracle_scene_desc* d, int32_t cap, int8_t* typ, double* pos,
+                          double* vel, double* nrm);
+/* its parameters: domain = tank, SetPara's umax / Pmax along gravity on z */
+int oracle_params_dambreak(const oracle_scene_desc* d, double snd, double dt, double knm_vsc,
+                           double g_z, int32_t precision, oracle_params* p);
+
 void* oracle_create(const oracle_params* p, int32_t n, const int8_t* typ, const void* pos,
                     const void* vel, const void* nrm);
 void oracle_destroy(void* h);

@@ -27,7 +27,21 @@ class oracle_params(C.Structure):
                 ("precision", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
+class oracle_scene_desc(C.Structure):
+    _fields_ = [("l0", C.c_double), ("tank", C.c_double * 3), ("block", C.c_int32 * 3),
+                ("wall_mask", C.c_int32), ("jitter", C.c_double), ("seed", C.c_uint64),
+                ("vel_sigma", C.c_double), ("vel_seed", C.c_uint64), ("origin", C.c_double * 3)]
+
+
+c_double_p = C.POINTER(C.c_double)
+
 SIGS = {
+    "oracle_scene_dambreak_count": (C.c_int, [C.POINTER(oracle_scene_desc), c_int32_p]),
+    "oracle_scene_dambreak": (C.c_int, [C.POINTER(oracle_scene_desc), C.c_int32, c_int8_p,
+                                        c_double_p, c_double_p, c_double_p]),
+    "oracle_params_dambreak": (C.c_int, [C.POINTER(oracle_scene_desc), C.c_double, C.c_double,
+                                         C.c_double, C.c_double, C.c_int32,
+                                         C.POINTER(oracle_params)]),
     "oracle_create": (C.c_void_p, [C.POINTER(oracle_params), C.c_int32, c_int8_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p]),
     "oracle_destroy": (None, [C.c_void_p]),
@@ -57,8 +71,8 @@ DIAG_COLUMNS = ["cell", "vsc_f", "vsc_m", "col_f", "col_w", "col_m", "prs_f", "p
 
 
 def build():
-    src = os.path.join(HERE, "mps_oracle.cpp")
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
+    srcs = [os.path.join(HERE, f) for f in ("mps_oracle.cpp", "oracle_scene.cpp", "mps_oracle.h")]
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(map(os.path.getmtime, srcs)):
         subprocess.run(["make", "-C", HERE, "libmps_oracle.so"], check=True, capture_output=True)
     return LIB
 

@@ -15,7 +15,9 @@
 # so this script is the whole recipe.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${MPS_REFERENCE_DIR:-/root/reference}"
+# the reference checkout: MPS_REFERENCE_DIR, else a directory named `reference` beside
+# this repository
+REF="${MPS_REFERENCE_DIR:-$(cd "$HERE/../.." && pwd)/reference}"
 OUT="$HERE/_ref"
 NVCC="${NVCC:-nvcc}"
 if [ ! -f "$REF/kernel.cu" ]; then

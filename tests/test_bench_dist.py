@@ -108,3 +108,33 @@ def test_reference_arm_under_two_ranks():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["value"] > 0 and d["n_gpus"] == 2
     assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_reference_arm_does_not_load_the_product():
+    """The reference arm builds its workload with the oracle's own scene generator: after a
+    run, neither the product package nor libmps_b200.so is loaded in its process, and its
+    `config` is the one the GPU arm prints for the same workload."""
+    import json
+    import subprocess
+    code = r"""
+import argparse, json, sys
+sys.path.insert(0, '.')
+import bench
+args = argparse.Namespace(workload='dambreak_l0.02_small', precision='f32', steps=2, warmup=1,
+                          gpus=1)
+bench.run_reference(args, 1, 0)
+maps = open('/proc/self/maps').read()
+print(json.dumps({'pkg': 'mps_cuda_b200' in sys.modules, 'so': 'libmps_b200' in maps}))
+"""
+    res = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                         timeout=600)
+    assert res.returncode == 0, res.stderr[-2000:]
+    lines = [json.loads(l) for l in res.stdout.splitlines() if l.startswith("{")]
+    line, loaded = lines[0], lines[-1]
+    assert loaded == {"pkg": False, "so": False}
+    import bench
+    from oracle import scenes
+    _, typ, _, _, _ = scenes.workload("dambreak_l0.02_small", "f32")
+    assert line["config"] == bench.bench_config("dambreak_l0.02_small", "f32",
+                                                int((typ == 0).sum()), int((typ != 0).sum()), 1)
+    assert line["steps"] == 2 and line["warmup"] == 1

@@ -1,29 +1,52 @@
-"""Size-independent properties at the 384k-particle dam break (l0 = 0.005), on the GPU.
+"""The benchmark workloads at their full size, on the GPU.
 
-The oracle is too slow at this size for step-by-step comparison, so these tests check what
-must hold at any size: the fused step equals the reference's method-by-method sequence
-bit for bit, runs are deterministic, particles are conserved, no counter reports an error,
-and the bucket lists come out sorted the way the step requires.
+Two fused steps of the 384 000-particle dam break (l0 = 0.005) are compared exactly with the
+oracle in FP32 and FP64, and two of the 6.1M-particle scene (l0 = 0.0025, FP32, the bench's
+headline workload) likewise; the oracle finishes those in seconds on the host's cores. Over
+more steps, properties that must hold at any size are checked: the fused step equals the
+reference's method-by-method sequence bit for bit, runs are deterministic, particles are
+conserved, no counter reports an error, and the bucket lists come out sorted the way the
+step requires. Every handle is closed when its test ends, so that full-size device memory
+is not held into the next test.
 """
 from __future__ import annotations
+
+import contextlib
 
 import numpy as np
 import pytest
 
-from mps_cuda_b200 import F32, MPS, configs, dambreak, dambreak_params
+from mps_cuda_b200 import F32, F64, MPS, configs, dambreak, dambreak_params
 from mps_cuda_b200 import _lib as L
 
 pytestmark = pytest.mark.gpu
 
 
+def _scene(workload, prec):
+    desc, dt, _ = configs.WORKLOADS[workload]
+    sc = dambreak(desc)
+    p = dambreak_params(desc, dt=dt, precision=prec)
+    rd = np.float64 if prec == F64 else np.float32
+    args = (sc["typ"], sc["pos"].astype(rd), sc["vel"].astype(rd), sc["nrm"].astype(rd))
+    return p, args
+
+
 @pytest.fixture(scope="module")
 def big():
-    desc, dt, _ = configs.WORKLOADS["dambreak_l0.005_384k"]
-    sc = dambreak(desc)
-    p = dambreak_params(desc, dt=dt, precision=F32)
-    args = (sc["typ"], sc["pos"].astype(np.float32), sc["vel"].astype(np.float32),
-            sc["nrm"].astype(np.float32))
-    return p, args
+    return _scene("dambreak_l0.005_384k", F32)
+
+
+@contextlib.contextmanager
+def handles(p, args, n):
+    """n solver handles on the same scene, closed on exit"""
+    hs = []
+    try:
+        for _ in range(n):
+            hs.append(MPS(p, *args))
+        yield hs
+    finally:
+        for h in hs:
+            h.close()
 
 
 def _same(a, b):
@@ -33,23 +56,23 @@ def _same(a, b):
 
 def test_fused_step_equals_method_sequence(big):
     p, args = big
-    fused, methods = MPS(p, *args), MPS(p, *args)
-    fused.set_option(L.OPT_GRAPH, 1)
-    fused.step(2)
-    for _ in range(2):
-        methods.step_by_methods()
-    _same(fused.state(), methods.state())
+    with handles(p, args, 2) as (fused, methods):
+        fused.set_option(L.OPT_GRAPH, 1)
+        fused.step(2)
+        for _ in range(2):
+            methods.step_by_methods()
+        _same(fused.state(), methods.state())
 
 
 def test_deterministic_and_conserving(big):
     p, args = big
-    a, b = MPS(p, *args), MPS(p, *args)
-    a.step(4)
-    b.step(2)
-    b.step(2)
-    sa, sb = a.state(), b.state()
+    with handles(p, args, 2) as (a, b):
+        a.step(4)
+        b.step(2)
+        b.step(2)
+        sa, sb = a.state(), b.state()
+        c = a.counters()
     _same(sa, sb)
-    c = a.counters()
     nf = int((args[0] == 0).sum())
     assert c["n_fluid_alive"] + c["n_deleted"] == nf == 384000
     assert c["err_mirror_slot"] == c["err_mirror_capacity"] == c["err_cell_range"] == c["err_nan"] == 0
@@ -61,10 +84,10 @@ def test_deterministic_and_conserving(big):
 
 def test_bucket_index_matches_positions(big):
     p, args = big
-    g = MPS(p, *args)
-    g.step(3)
-    st, d = g.state(), g.diag()
-    inf = g.info()
+    with handles(p, args, 1) as (g,):
+        g.step(3)
+        st, d = g.state(), g.diag()
+        inf = g.info()
     x = st["pos"].astype(np.float32)
     minc = np.array(inf.minc, np.float32)
     dbinv = np.float32(inf.dbinv)
@@ -77,28 +100,55 @@ def test_bucket_index_matches_positions(big):
 
 def test_skipping_bucket_rows_changes_nothing(big):
     p, args = big
-    a, b = MPS(p, *args), MPS(p, *args)
-    b.set_option(L.OPT_CELL_SKIP, 0)
-    a.step(2)
-    b.step(2)
-    _same(a.state(), b.state())
+    with handles(p, args, 2) as (a, b):
+        b.set_option(L.OPT_CELL_SKIP, 0)
+        a.step(2)
+        b.step(2)
+        _same(a.state(), b.state())
+
+
+def _steps_equal_oracle(p, args, min_mirrors):
+    from oracle.oracle import Oracle, params_from
+    o = Oracle(params_from(p), *args)
+    try:
+        with handles(p, args, 1) as (g,):
+            g.set_option(L.OPT_GRAPH, 1)
+            g.step(2)
+            a = g.state()
+            gm = g.mirrors(2)
+            c = g.counters()
+        o.step(2)
+        b = o.state()
+        for k in ("typ", "pos", "vel", "prs", "pav"):
+            assert np.array_equal(a[k], b[k]), k
+        om = o.mirrors()
+        assert len(gm["slot"]) > min_mirrors
+        assert np.array_equal(gm["slot"], om["slot"]) and np.array_equal(gm["pos"], om["pos"])
+        assert np.array_equal(gm["prs"], om["prs"])
+        assert c["err_mirror_slot"] == c["err_mirror_capacity"] == c["err_cell_range"] == 0
+        assert c["err_nan"] == 0
+    finally:
+        o.close()
 
 
 def test_full_size_steps_equal_the_oracle(big):
-    """At the benchmark's own size (384 000 fluid particles, FP32) two fused steps give the
-    oracle's state exactly, mirrors included."""
-    from oracle.oracle import Oracle, params_from
+    """At the 384k workload's own size (384 000 fluid particles, FP32) two fused steps give
+    the oracle's state exactly, mirrors included."""
     p, args = big
-    g = MPS(p, *args)
-    o = Oracle(params_from(p), *args)
-    try:
-        g.step(2)
-        o.step(2)
-        a, b = g.state(), o.state()
-        for k in ("typ", "pos", "vel", "prs", "pav"):
-            assert np.array_equal(a[k], b[k]), k
-        gm, om = g.mirrors(2), o.mirrors()
-        assert len(gm["slot"]) > 80000
-        assert np.array_equal(gm["slot"], om["slot"]) and np.array_equal(gm["pos"], om["pos"])
-    finally:
-        g.close()
+    _steps_equal_oracle(p, args, 80000)
+
+
+def test_full_size_f64_steps_equal_the_oracle():
+    """The same at 384 000 particles in FP64 (the reference's commented `typedef double
+    real`, const.cuh:53)."""
+    p, args = _scene("dambreak_l0.005_384k", F64)
+    _steps_equal_oracle(p, args, 80000)
+
+
+def test_largest_scene_steps_equal_the_oracle():
+    """The headline workload: 6 144 000 fluid and 614 400 wall particles (l0 = 0.0025, FP32,
+    bucket rebuild every step). Two fused steps equal the oracle's exactly, state and the
+    second mirror generation."""
+    p, args = _scene("dambreak_l0.0025_6.1M", F32)
+    assert int((args[0] == 0).sum()) == 6144000
+    _steps_equal_oracle(p, args, 300000)

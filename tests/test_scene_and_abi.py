@@ -61,6 +61,36 @@ def test_argument_errors_without_gpu():
     assert lib.mps_destroy(None) == L.MPS_OK
 
 
+@pytest.mark.parametrize("prec", [F32, F64])
+def test_grid_too_large_for_int32_cells_is_rejected_before_any_device_use(prec):
+    """A domain whose bucket grid does not fit int32 fine-cell indices is refused by the host
+    arithmetic (64-bit bucket counts), by mps_derive, mps_create and the no-allocation
+    bucket build alike, before any device is touched (this runs without a GPU)."""
+    lib = L.lib()
+    desc = SceneDesc(0.02, (0.4, 0.2, 0.4), (2, 2, 2))
+    sc = dambreak(desc)
+    for ext in ((2000.0, 2000.0, 2000.0), (1e9, 1.0, 1.0)):
+        p = dambreak_params(desc, precision=prec, max=ext)
+        inf = L.mps_info()
+        assert lib.mps_derive(C.byref(p), C.byref(inf)) == L.MPS_ERR_OVERFLOW
+        assert b"bucket" in lib.mps_last_error()
+        h = C.c_void_p()
+        n = sc["typ"].shape[0]
+        rd = np.float64 if prec == F64 else np.float32
+        arr = [np.ascontiguousarray(sc[k], rd) for k in ("pos", "vel", "nrm")]
+        rc = lib.mps_create(C.byref(p), n, sc["typ"].ctypes.data_as(L.c_int8_p),
+                            *(a.ctypes.data_as(C.c_void_p) for a in arr), C.byref(h))
+        assert rc == L.MPS_ERR_OVERFLOW and not h.value
+        start = np.zeros(4, np.int32)  # host memory: the call must return before using it
+        rc = lib.mps_bucket_build_noalloc(C.byref(p), 0, None, None, None, None,
+                                          start.ctypes.data_as(C.c_void_p), None)
+        assert rc == L.MPS_ERR_OVERFLOW
+        assert np.all(start == 0)
+    # a grid that fits is still accepted
+    p = dambreak_params(desc, precision=prec)
+    assert lib.mps_derive(C.byref(p), C.byref(L.mps_info())) == L.MPS_OK
+
+
 def _has_gpu():
     try:
         import torch

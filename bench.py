@@ -74,6 +74,54 @@ def alg_bytes(group: str, s: int, nf: int, m1: int, m2: int) -> float:
     }[group]
 
 
+# Arithmetic of the neighbour passes per unit of work (flops count a fused multiply-add as
+# 2; square roots and divisions apart, since they cost several instructions each):
+#   candidate test, list entry : dx, dy, dz and dot3                      8 flops
+#   VscTrm pair                : d2 * d, u_j - u_i, 3 fma, sqrt, 2 l0 / t  10 flops, 1 sqrt, 1 div
+#   ChkCol hit                 : u_i - u_j, dot3, f * (colfac / d2), 3 fma  15 flops, 1 div
+#   MkPrs pair                 : sqrt, re/d - d/re                          1 flop, 1 sqrt, 2 div
+#   PrsGrdTrm pair             : sqrt, (re/d - d/re) / d2, P_j - P_min,
+#                                 (P_j - P_min) w, 3 fma                     9 flops, 1 sqrt, 3 div
+# (kernel.cu:1062-1064, 1215-1220, 1346-1348, 1730-1735)
+def pair_arith(work: dict, diag: dict) -> dict:
+    """Per kernel group: (flops, square roots, divisions) of one step from the device's own
+    counts (mps_get_work, mps_get_diag) of that step."""
+    s = {k: float(np.sum(v, dtype=np.int64)) for k, v in diag.items() if k != "ndens"}
+    va = s["vsc_f"] + s["vsc_m"]
+    col = s["col_f"] + s["col_w"] + s["col_m"]
+    prs = s["prs_f"] + s["prs_m"]
+    grd = s["grd_f"] + s["grd_m"]
+    n_list = float(work["list_entries"])
+    return {
+        "pass_a": (8 * float(work["visc_candidates"]) + 10 * va, va, va),
+        "pass_b": (8 * float(work["list_candidates"]) + 8 * n_list + 15 * col + prs, prs,
+                   col + 2 * prs),
+        "pass_c": (16 * n_list + 9 * grd, grd, 3 * grd),
+    }
+
+
+def compute_roofline(ops, ms: float, ar: dict, f64: bool) -> dict:
+    """Bound of one launch by the measured arithmetic rates: its flops at the fused
+    multiply-add rate plus its square roots and divisions at theirs (they share the
+    issue slots, so the times add)."""
+    flops, nsq, ndv = ops
+    pre = "fp64" if f64 else "fp32"
+    t = (flops / ar[f"{pre}_fma_flops"] + nsq / ar[f"{pre}_sqrt_per_s"]
+         + ndv / ar[f"{pre}_div_per_s"])
+    ach = flops / (ms / 1e3)
+    return {"flops_per_launch": flops, "sqrt_per_launch": nsq, "div_per_launch": ndv,
+            "achieved_flops": ach, "flop_frac": ach / ar[f"{pre}_fma_flops"],
+            "arith_bound_ms": 1e3 * t, "arith_frac": 1e3 * t / ms}
+
+
+def issue_active(workload: str, precision: str):
+    """Issue-active fraction per kernel group from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "issue_active.json")
+    if not os.path.exists(p):
+        return {}
+    return json.load(open(p)).get(f"{workload}:{precision}", {})
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -376,6 +424,32 @@ def run_ours(args, world, rank, local):
                 "alg_bytes_per_launch": groups[dom]["alg_bytes"],
                 "ms_per_launch": groups[dom]["ms_per_launch"]}
 
+    # ---- companion compute roofline: the passes' pair arithmetic against the device's
+    # own measured FMA / sqrt / division rates, from one more step run with the device
+    # counting its work (after the timed region) --------------------------------------
+    compute = None
+    if not args.no_compute:
+        from mps_cuda_b200 import measure_arith
+        ar = measure_arith()
+        w0 = g.work()
+        g.set_option(L.OPT_DIAG, 1)
+        g.step(1)
+        g.set_option(L.OPT_DIAG, 0)
+        w1 = g.work()
+        ops = pair_arith({k: w1[k] - w0[k] for k in w1}, g.diag())
+        ia = issue_active(args.workload, args.precision)
+        compute = {"arith_peaks": ar, "issue_active_source": "profiles/issue_active.json (ncu)",
+                   "groups": {}}
+        for k_, o_ in ops.items():
+            if k_ in groups:
+                compute["groups"][k_] = compute_roofline(o_, groups[k_]["ms_per_launch"], ar,
+                                                         args.precision == "f64")
+                compute["groups"][k_]["issue_active"] = ia.get(k_)
+        if dom in compute["groups"]:
+            roofline["flop_frac"] = compute["groups"][dom]["flop_frac"]
+            roofline["arith_frac"] = compute["groups"][dom]["arith_frac"]
+            roofline["issue_active"] = compute["groups"][dom]["issue_active"]
+
     # ---- end to end through the C-ABI with pinned host buffers --------------------------
     e2e = None
     if not args.no_e2e:
@@ -441,7 +515,8 @@ def run_ours(args, world, rank, local):
             "graph": True,
             "clocks": clk.summary(), "wall_ms_per_step": 1e3 * wall / K,
             "e2e": e2e, "gpu_launches": launches,
-            "roofline": roofline, "kernel_groups": groups, "cpu_baseline": cpu,
+            "roofline": roofline, "compute_roofline": compute, "kernel_groups": groups,
+            "cpu_baseline": cpu,
             "batched": batched,
             "adjoint": adjoint,
             "other_workloads": extra,
@@ -650,6 +725,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-extra", action="store_true")
+    ap.add_argument("--no-compute", action="store_true")
     args = ap.parse_args()
     world, rank, local = setup_dist()
     try:

@@ -108,7 +108,9 @@ typedef struct mps_counters {
     int32_t err_nan;               /* non-finite position met in a bucket build             */
     int32_t reserved0;
     int64_t kernel_launches;       /* kernels this handle launched (graph replays included) */
-    int32_t reserved[2];
+    int32_t stage_blocks;          /* with MPS_OPT_DIAG and staging: blocks of VscTrm that
+                                      walked shared memory (cumulative)                     */
+    int32_t unstaged_blocks;       /* ... and blocks whose neighbourhood did not fit        */
 } mps_counters;
 
 /* Per-particle diagnostic counters (mps_get_diag), column order of the int32 table. */
@@ -152,12 +154,22 @@ enum {
     MPS_OPT_TIMING = 4,      /* 1: time every kernel group of mps_step with CUDA events
                                 on the handle's stream (steps then run without a graph) */
     MPS_OPT_GRADIENT = 5,    /* PrsGrdTrm variant, MPS_GRAD_* (default STANDARD)        */
-    MPS_OPT_LIST_CAPACITY = 6 /* neighbour-list entries kept per particle between ChkCol/
+    MPS_OPT_LIST_CAPACITY = 6, /* neighbour-list entries kept per particle between ChkCol/
                                 MkPrs and PrsGrdTrm: 0 or above 160 = 160 (the default).
                                 A particle with more neighbours walks its fine cells again
                                 instead, with the same result; lower values exercise that
                                 path. Changing it voids a recorded adjoint rollout.       */
+    MPS_OPT_STAGING = 7,     /* where VscTrm's candidate walk reads: MPS_STAGE_*         */
+    MPS_OPT_STAGE_CAPACITY = 8 /* candidates a block may stage in shared memory (0 = the
+                                default); a block whose neighbourhood holds more walks
+                                global memory. Results never depend on it.               */
 };
+
+/* MPS_OPT_STAGING. GLOBAL: each particle walks its fine cells through L1. POSITIONS: a block
+ * first copies its particles' neighbourhood (the fine rows their walks reach) into shared
+ * memory and walks it there. VELOCITIES: also the candidates' velocities. The candidates
+ * and their order are the same in all three, so results are identical. */
+enum { MPS_STAGE_GLOBAL = 0, MPS_STAGE_POSITIONS = 1, MPS_STAGE_VELOCITIES = 2 };
 
 /* PrsGrdTrm variants (MPS_OPT_GRADIENT). STANDARD is the kernel the reference compiles
  * (kernel.cu:1651-1794). CORRECTED is its `#if 0` alternative (kernel.cu:1435-1648): the
@@ -438,6 +450,34 @@ int mps_output_close(mps_output* o);
  */
 int mps_bucket_build_noalloc(const mps_params* p, int32_t n, const int8_t* typ, const void* pos,
                              int32_t* cell, int32_t* order, int32_t* start, void* stream);
+
+/* ---- measurement ------------------------------------------------------------------ */
+/* Work of the neighbour passes, counted on the device during the steps run with
+ * MPS_OPT_DIAG (cumulative over the handle's life). The neighbour pairs themselves are the
+ * columns of mps_get_diag. No counterpart in the reference. */
+typedef struct mps_work {
+    int64_t visc_candidates;  /* fluid candidates VscTrm's walk tested                   */
+    int64_t list_candidates;  /* fluid candidates tested to build ChkCol/MkPrs's lists   */
+    int64_t list_entries;     /* entries of those lists (read once by ChkCol/MkPrs, twice
+                                 by PrsGrdTrm)                                           */
+    int64_t reserved[5];
+} mps_work;
+int mps_get_work(mps_handle* h, mps_work* out);
+
+/* Arithmetic throughput of the current device, measured by project-written micro-kernels
+ * (eight independent chains per thread on every SM, CUDA events, best of three): the
+ * denominators of the neighbour passes' compute roofline. A square root or division is
+ * counted with the one dependent addition its chain needs. No counterpart in the
+ * reference. */
+typedef struct mps_arith {
+    double fp32_fma_flops, fp64_fma_flops;    /* 2 flops per fused multiply-add       */
+    double fp32_sqrt_per_s, fp32_div_per_s;   /* IEEE sqrt / division (round to nearest) */
+    double fp64_sqrt_per_s, fp64_div_per_s;
+    double warp_issue_per_s;                  /* 4 schedulers per SM at the rated clock */
+    int32_t sms, clock_khz;
+    double reserved[4];
+} mps_arith;
+int mps_measure_arith(mps_arith* out);
 
 /* ---- errors ----------------------------------------------------------------------- */
 const char* mps_status_string(int32_t status);

@@ -32,6 +32,8 @@ F32, F64, F32_N64 = 0, 1, 2
  PHASE_VSCTRM, PHASE_UPPCL1, PHASE_CHKCOL, PHASE_MKPRS, PHASE_PRSGRDTRM, PHASE_UPPCL2) = range(11)
 OPT_DIAG, OPT_GRAPH, OPT_BLOCK, OPT_CELL_SKIP, OPT_TIMING, OPT_GRADIENT = 0, 1, 2, 3, 4, 5
 OPT_LIST_CAPACITY = 6
+OPT_STAGING, OPT_STAGE_CAPACITY = 7, 8
+STAGE_GLOBAL, STAGE_POSITIONS, STAGE_VELOCITIES = 0, 1, 2
 GRAD_STANDARD, GRAD_CORRECTED = 0, 1
 KERNEL_GROUPS = ["pass_a", "pass_b", "pass_c", "gen_cull", "bin_fluid", "bin_mirror"]
 DIAG_COLUMNS = ["cell", "vsc_f", "vsc_m", "col_f", "col_w", "col_m", "prs_f", "prs_m",
@@ -63,7 +65,20 @@ class mps_counters(C.Structure):
                 ("err_mirror_slot", C.c_int32), ("err_mirror_capacity", C.c_int32),
                 ("err_cell_range", C.c_int32), ("err_nan", C.c_int32),
                 ("reserved0", C.c_int32), ("kernel_launches", C.c_int64),
-                ("reserved", C.c_int32 * 2)]
+                ("stage_blocks", C.c_int32), ("unstaged_blocks", C.c_int32)]
+
+
+class mps_work(C.Structure):
+    _fields_ = [("visc_candidates", C.c_int64), ("list_candidates", C.c_int64),
+                ("list_entries", C.c_int64), ("reserved", C.c_int64 * 5)]
+
+
+class mps_arith(C.Structure):
+    _fields_ = [("fp32_fma_flops", C.c_double), ("fp64_fma_flops", C.c_double),
+                ("fp32_sqrt_per_s", C.c_double), ("fp32_div_per_s", C.c_double),
+                ("fp64_sqrt_per_s", C.c_double), ("fp64_div_per_s", C.c_double),
+                ("warp_issue_per_s", C.c_double), ("sms", C.c_int32), ("clock_khz", C.c_int32),
+                ("reserved", C.c_double * 4)]
 
 
 class mps_physical(C.Structure):
@@ -108,6 +123,8 @@ SIGNATURES = {
                                   C.c_void_p, c_int32_p]),
     "mps_get_diag": (C.c_int, [C.c_void_p, c_int32_p, C.c_void_p]),
     "mps_get_counters": (C.c_int, [C.c_void_p, C.POINTER(mps_counters)]),
+    "mps_get_work": (C.c_int, [C.c_void_p, C.POINTER(mps_work)]),
+    "mps_measure_arith": (C.c_int, [C.POINTER(mps_arith)]),
     "mps_get_timing": (C.c_int, [C.c_void_p, C.c_int32, c_double_p, C.POINTER(C.c_int64),
                                  C.c_int32]),
     "mps_autotune": (C.c_int, [C.c_void_p, C.c_int32, c_int32_p]),

@@ -21,7 +21,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmps_b200.so")
 SOURCES = ["mps_api.cu", "mps_inst_f32.cu", "mps_inst_f64.cu", "mps_inst_mix.cu",
-           "mps_noalloc.cu", "mps_scene.cpp", "mps_io.cpp", "mps_output.cu"]
+           "mps_noalloc.cu", "mps_scene.cpp", "mps_io.cpp", "mps_output.cu", "mps_peaks.cu"]
 HEADERS = ["mps_types.h", "mps_device.cuh", "mps_kernels.cuh", "mps_adjoint.cuh", "mps_solver.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -174,6 +174,18 @@ int mps_set_option(mps_handle* h, int32_t opt, int32_t value) {
                 if (value < 0) throw ApiError(MPS_ERR_ARG, "list capacity must not be negative");
                 s.set_list_capacity(value);
                 break;
+            case MPS_OPT_STAGING:
+                if (value < MPS_STAGE_GLOBAL || value > MPS_STAGE_VELOCITIES)
+                    throw ApiError(MPS_ERR_ARG, "staging must be one of MPS_STAGE_*");
+                s.stage_mode = value;
+                s.invalidate_graph();
+                break;
+            case MPS_OPT_STAGE_CAPACITY:
+                if (value < 0 || value > (1 << 16))
+                    throw ApiError(MPS_ERR_ARG, "stage capacity must lie in [0, 65536]");
+                s.stage_cap = value;
+                s.invalidate_graph();
+                break;
             case MPS_OPT_GRADIENT:
                 if (value != MPS_GRAD_STANDARD && value != MPS_GRAD_CORRECTED)
                     throw ApiError(MPS_ERR_ARG, "gradient must be MPS_GRAD_STANDARD or _CORRECTED");
@@ -244,6 +256,11 @@ int mps_get_diag(mps_handle* h, int32_t* table, void* ndens) {
 int mps_get_counters(mps_handle* h, mps_counters* out) {
     if (!out) return fail(MPS_ERR_ARG, "null buffer");
     return guarded(h, [&](SolverBase& s) { s.get_counters(out); });
+}
+
+int mps_get_work(mps_handle* h, mps_work* out) {
+    if (!out) return fail(MPS_ERR_ARG, "null buffer");
+    return guarded(h, [&](SolverBase& s) { s.get_work(out); });
 }
 
 int mps_get_timing(mps_handle* h, int32_t kernel, double* total_ms, int64_t* launches,

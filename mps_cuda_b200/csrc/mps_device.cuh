@@ -145,14 +145,17 @@ __device__ __forceinline__ int fine_rowmajor(const SceneDev<R, RN>& sc, int c) {
 // (radius + margin)^2, the margin (1e-3 of a bucket) covering the float geometry. The
 // neighbours inside the radius, and their order, are those of a walk over every fine cell
 // of the 27 buckets.
-template <class R, class RN, class F>
-__device__ __forceinline__ void for_fluid_ranges(const SceneDev<R, RN>& sc,
-                                                 const int* __restrict__ csr, const RowCtx<R>& c,
-                                                 R B, F&& f) {
+// The fine rows of that walk: g(fz, fy, xl, xh) for every fine row (fz, fy) within sqrt(B),
+// z then y ascending, with the fine cells [xl, xh] of the row it reaches. Every step is
+// monotone in the particle's coordinates (IEEE arithmetic, clamps, truncation), which the
+// staged walk relies on to bound the rows of a whole block from the box around its
+// particles (stage_fluid).
+template <class R, class RN, class G>
+__device__ __forceinline__ void for_fluid_rows(const SceneDev<R, RN>& sc, const RowCtx<R>& c, R B,
+                                               G&& g) {
     const float b = float(B), hf = sc.hf, ih = sc.ihf;
     const float s = sqrtf(b);
     const int fx0 = 3 * c.ix - 3, fy0 = 3 * c.iy - 3, fz0 = 3 * c.iz - 3;
-    const int nfx = 3 * sc.nbx, nfxy = 9 * sc.nbxy;
     const int zl = fine_at(c.rz - s, ih, fz0), zh = fine_at(c.rz + s, ih, fz0);
     for (int fz = zl; fz <= zh; ++fz) {
         const float gz = fine_gap(c.rz, fz, hf);
@@ -161,11 +164,20 @@ __device__ __forceinline__ void for_fluid_ranges(const SceneDev<R, RN>& sc,
         for (int fy = yl; fy <= yh; ++fy) {
             const float gy = fine_gap(c.ry, fy, hf);
             const float sx = sqrtf(fmaxf(bz - gy * gy, 0.0f));
-            const int xl = fine_at(c.rx - sx, ih, fx0), xh = fine_at(c.rx + sx, ih, fx0);
-            const int row = sc.fbase + fz * nfxy + fy * nfx;
-            f(__ldg(csr + row + xl), __ldg(csr + row + xh + 1));
+            g(fz, fy, fine_at(c.rx - sx, ih, fx0), fine_at(c.rx + sx, ih, fx0));
         }
     }
+}
+
+template <class R, class RN, class F>
+__device__ __forceinline__ void for_fluid_ranges(const SceneDev<R, RN>& sc,
+                                                 const int* __restrict__ csr, const RowCtx<R>& c,
+                                                 R B, F&& f) {
+    const int nfx = 3 * sc.nbx, nfxy = 9 * sc.nbxy;
+    for_fluid_rows(sc, c, B, [&](int fz, int fy, int xl, int xh) {
+        const int row = sc.fbase + fz * nfxy + fy * nfx;
+        f(__ldg(csr + row + xl), __ldg(csr + row + xh + 1));
+    });
 }
 
 template <class R, class RN, class F>

@@ -14,6 +14,7 @@
 // Mirrors produced by pass C are the next step's first generation: GenMRR at the start of
 // the next step (kernel.cu:1906-1908) would read the same positions and pressures.
 #pragma once
+#include <climits>
 #include <type_traits>
 
 #include "mps_device.cuh"
@@ -527,14 +528,16 @@ __device__ __forceinline__ const SceneDev<R, RN>& scene_ref(const PassArgs<R, RN
 
 // Phase 1 of a neighbour pass: the fluid neighbours j != s with d2 <= thr, in visiting
 // order, into the slot's list. Returns the neighbour count (may exceed nbK).
-template <class R, class RN>
+template <class R, class RN, bool COUNT = false>
 __device__ __forceinline__ int build_list(const PassArgs<R, RN>& a, const SceneDev<R, RN>& sc,
-                                          const RowCtx<R>& c, int s, R x, R y, R z, R thr, R B) {
+                                          const RowCtx<R>& c, int s, R x, R y, R z, R thr, R B,
+                                          int* ncand = nullptr) {
     int cnt = 0;
     int* __restrict__ nb = a.nb;
     const V4<R>* __restrict__ posf = a.posf;
     const int nF = a.nF, K = a.nbK;
     for_fluid_ranges(sc, a.csr, c, B, [&](int lo, int hi) {
+        if (COUNT) *ncand += hi - lo;
         // four independent loads in flight before the first test (latency, not bandwidth,
         // bounds this loop), a short row's included: past the row's end the particle itself
         // pads the batch and visit() rejects it; candidates are tested and appended in
@@ -562,6 +565,185 @@ __device__ __forceinline__ int build_list(const PassArgs<R, RN>& a, const SceneD
     return cnt;
 }
 
+// ---------------------------------------------------------------------------------------
+// shared-memory staging of a block's fluid neighbourhood
+// ---------------------------------------------------------------------------------------
+// A block's slots are consecutive in bucket-major order, so its particles lie in a few
+// x-adjacent buckets, and the candidates all of them visit lie in a small set of fine rows.
+// stage_fluid copies those rows' ranges of posf (contiguous per fine row) into shared memory
+// with coalesced warp loads, optionally with each candidate's velocity gathered once for the
+// whole block, and builds a table of the staged index of every fine cell start. Each
+// particle then walks its own rows (for_fluid_rows, the same geometry as the global walk)
+// out of shared memory: the same candidates in the same order, so the sums are unchanged.
+//
+// The staged rows are the union of the particles' fine planes (exact, from their own walk
+// bounds) and, per row, the fine x range reached from the box around the particles' float
+// coordinates. Every step of the row geometry is monotone in the coordinates, so a box
+// corner is never nearer than a particle inside it and the box range covers each
+// particle's own range for that row. Blocks whose rows do not fit (particles in two bucket
+// rows, more than kStageSpan buckets along x, or more candidates than the staging
+// capacity) walk global memory instead, decided uniformly for the block.
+constexpr int kStageRows = 81;                     // 9 x 9 fine rows
+constexpr int kStageSpan = 8;                      // buckets along x, max - min
+constexpr int kStageCols = 3 * kStageSpan + 10;    // fine cells [3 ix_min - 3, 3 ix_max + 5] + end
+
+struct StageHdr {
+    int zl, zh, yl, yh;        // union of the particles' fine planes and widest fine rows
+    int ixl, ixh;              // bucket x range of the particles
+    unsigned box[6];           // x0, x1, y0, y1, z0, z1 as order-preserving integers
+    int smin, smax;            // scenes of the particles
+    int nrow, ny, fx0, ncol;   // rows staged, rows per plane, first fine x, table columns
+    int total;                 // candidates staged
+    int xl[kStageRows], xh[kStageRows];  // fine x range staged per row
+    int rs[kStageRows];        // posf index of each row's first staged candidate
+    int base[kStageRows + 1];  // staged index of each row's first candidate
+    int tab[kStageRows * kStageCols];  // staged index of each fine cell start
+};
+
+__device__ __forceinline__ unsigned ord_bits(float f) {
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord_float(unsigned u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+// distance from [v0, v1] to fine cell f along one axis (fine_gap of the nearer end)
+__device__ __forceinline__ float fine_gap_box(float v0, float v1, int f, float hf) {
+    const float lo = float(f - 3) * hf;
+    return fmaxf(fmaxf(lo - v1, v0 - (lo + hf)), 0.0f);
+}
+
+template <class R> __host__ __device__ constexpr size_t stage_smem_bytes(int cap, bool vel) {
+    return ((sizeof(StageHdr) + 15) / 16) * 16 + size_t(cap) * sizeof(V4<R>) * (vel ? 2 : 1);
+}
+
+// Stage the block's neighbourhood (every thread of the block calls this). `act`: this
+// thread holds a particle of scene `scene` whose walk context is `c`; bsel(scene) gives the
+// walk bound B (radius plus margin, squared) of the pass. Returns true (uniformly) when the
+// stage was built; spos (and svel) then hold the candidates.
+template <class R, class RN, bool SVEL, class BSel>
+__device__ bool stage_fluid(const PassArgs<R, RN>& a, StageHdr& h, V4<R>* spos, V4<R>* svel,
+                            int cap, bool act, int scene, const RowCtx<R>& c, BSel&& bsel) {
+    const int tid = threadIdx.x, nth = blockDim.x;
+    if (tid == 0) {
+        h.zl = h.yl = h.ixl = h.smin = INT_MAX;
+        h.zh = h.yh = h.ixh = h.smax = INT_MIN;
+        h.box[0] = h.box[2] = h.box[4] = 0xffffffffu;
+        h.box[1] = h.box[3] = h.box[5] = 0u;
+    }
+    __syncthreads();
+    if (act) {
+        const SceneDev<R, RN>& sc = a.sc[scene];
+        const float b = float(bsel(sc)), ih = sc.ihf, s = sqrtf(b);
+        atomicMin(&h.zl, fine_at(c.rz - s, ih, 3 * c.iz - 3));
+        atomicMax(&h.zh, fine_at(c.rz + s, ih, 3 * c.iz - 3));
+        atomicMin(&h.yl, fine_at(c.ry - s, ih, 3 * c.iy - 3));
+        atomicMax(&h.yh, fine_at(c.ry + s, ih, 3 * c.iy - 3));
+        atomicMin(&h.ixl, c.ix);
+        atomicMax(&h.ixh, c.ix);
+        atomicMin(&h.box[0], ord_bits(c.rx));
+        atomicMax(&h.box[1], ord_bits(c.rx));
+        atomicMin(&h.box[2], ord_bits(c.ry));
+        atomicMax(&h.box[3], ord_bits(c.ry));
+        atomicMin(&h.box[4], ord_bits(c.rz));
+        atomicMax(&h.box[5], ord_bits(c.rz));
+        atomicMin(&h.smin, scene);
+        atomicMax(&h.smax, scene);
+    }
+    __syncthreads();
+    if (h.smax < 0 || h.smin != h.smax) return false;
+    const int ny = h.yh - h.yl + 1, nrow = (h.zh - h.zl + 1) * ny;
+    if (nrow > kStageRows || h.ixh - h.ixl > kStageSpan) return false;
+    const SceneDev<R, RN>& sc = a.sc[h.smin];
+    const int fx0 = 3 * h.ixl - 3, ncol = 3 * (h.ixh - h.ixl) + 10;
+    const int nfx = 3 * sc.nbx, nfxy = 9 * sc.nbxy;
+    // the fine x range of each row reached from the box of the particles
+    for (int r = tid; r < nrow; r += nth) {
+        const int fz = h.zl + r / ny, fy = h.yl + r % ny;
+        const float b = float(bsel(sc)), hf = sc.hf, ih = sc.ihf;
+        const float gz = fine_gap_box(ord_float(h.box[4]), ord_float(h.box[5]), fz, hf);
+        const float bz = fmaxf(b - gz * gz, 0.0f);
+        const float gy = fine_gap_box(ord_float(h.box[2]), ord_float(h.box[3]), fy, hf);
+        const float sx = sqrtf(fmaxf(bz - gy * gy, 0.0f));
+        const float lo = fmaf(ord_float(h.box[0]) - sx, ih, 3.0f);
+        const float hi = fmaf(ord_float(h.box[1]) + sx, ih, 3.0f);
+        const int fxh = 3 * h.ixh - 3;
+        h.xl[r] = int(fminf(fmaxf(lo, float(fx0)), float(fx0 + 8)));
+        h.xh[r] = int(fminf(fmaxf(hi, float(fxh)), float(fxh + 8)));
+    }
+    __syncthreads();
+    // raw posf index of the fine cell starts the rows' ranges need
+    for (int e = tid; e < nrow * ncol; e += nth) {
+        const int r = e / ncol, k = e - r * ncol;
+        if (k >= h.xl[r] - fx0 && k <= h.xh[r] + 1 - fx0) {
+            const int fz = h.zl + r / ny, fy = h.yl + r % ny;
+            h.tab[r * ncol + k] = __ldg(a.csr + sc.fbase + fz * nfxy + fy * nfx + fx0 + k);
+        }
+    }
+    __syncthreads();
+    if (tid < 32) {  // staged bases: exclusive scan of the row counts in row order
+        const int lane = tid, per = (nrow + 31) / 32;
+        int sum = 0;
+        for (int q = 0; q < per; ++q) {
+            const int r = lane * per + q;
+            if (r < nrow) {
+                const int lo = h.tab[r * ncol + h.xl[r] - fx0];
+                h.rs[r] = lo;
+                sum += h.tab[r * ncol + h.xh[r] + 1 - fx0] - lo;
+            }
+        }
+        int inc = sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += v;
+        }
+        int run = inc - sum;
+        for (int q = 0; q < per; ++q) {
+            const int r = lane * per + q;
+            if (r < nrow) {
+                h.base[r] = run;
+                run += h.tab[r * ncol + h.xh[r] + 1 - fx0] - h.rs[r];
+            }
+        }
+        if (lane == 31) {
+            h.base[nrow] = inc;
+            h.total = inc;
+            h.nrow = nrow;
+            h.ny = ny;
+            h.fx0 = fx0;
+            h.ncol = ncol;
+        }
+    }
+    __syncthreads();
+    if (h.total > cap) return false;
+    for (int e = tid; e < nrow * ncol; e += nth) {
+        const int r = e / ncol, k = e - r * ncol;
+        if (k >= h.xl[r] - fx0 && k <= h.xh[r] + 1 - fx0)
+            h.tab[r * ncol + k] = h.base[r] + (h.tab[r * ncol + k] - h.rs[r]);
+    }
+    const int lane = tid & 31;
+    for (int r = tid >> 5; r < nrow; r += nth >> 5) {
+        const int n = h.base[r + 1] - h.base[r];
+        const V4<R>* __restrict__ src = a.posf + h.rs[r];
+        V4<R>* dst = spos + h.base[r];
+        for (int k = lane; k < n; k += 32) {
+            const V4<R> q = ldg4(src + k);
+            dst[k] = q;
+            if (SVEL) svel[h.base[r] + k] = ldg4(a.vel + w_slot(q.w));
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
+// the staged range [lo, hi) of fine row (fz, fy), cells [xl, xh]
+__device__ __forceinline__ void staged_range(const StageHdr& h, int fz, int fy, int xl, int xh,
+                                             int& lo, int& hi) {
+    const int* t = h.tab + ((fz - h.zl) * h.ny + (fy - h.yl)) * h.ncol - h.fx0;
+    lo = t[xl];
+    hi = t[xh + 1];
+}
+
 // state of a slot in a recorded step, kept in the w component of the pre-clamp velocity
 constexpr int kTapeOk = 0, kTapeClamped = 1, kTapeDeleted = 2, kTapeDead = 3;
 
@@ -577,77 +759,71 @@ __device__ __forceinline__ void tape_record(const PassArgs<R, RN>& a, const Scen
     a.tape_pre[s] = V4<R>{ux, uy, uz, R(st)};
 }
 
-// pass A: VscTrm (kernel.cu:1013-1119) + UpPcl1/ChkPcl (kernel.cu:1138-1149, 481-513).
-// TAPE (recorded rollouts): also keeps the list length and the velocity before the clamp.
-template <class R, class RN, bool DIAG, bool TAPE = false>
-__global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.nF) return;
-    const int nalive = __ldg(a.cs + a.dead);
-    if (s >= nalive) {  // unlisted particles are carried over unchanged
-        a.tpos[s] = a.pos[s];
-        a.tvel[s] = a.vel[s];
-        a.ttyp[s] = a.typ[s];
-        if (TAPE) {
-            a.tape_pre[s] = V4<R>{R(0), R(0), R(0), R(kTapeDead)};
-            a.nbcnt[s] = 0;
+// Pass A's candidate walk for one particle: each candidate tested, then the velocity term of
+// each neighbour in visiting order; four candidates' positions and the accepted ones'
+// velocities in flight at a time. ranges(f) hands the candidate ranges [lo, hi) to f in
+// visiting order; cand(k) is candidate k's position (w = slot), velo(k, j) the velocity of
+// candidate k (slot j). TAPE: the neighbours' slots also go to the slot's list.
+template <class R, class RN, bool TAPE, bool COUNT, class Ranges, class Cand, class Velo>
+__device__ __forceinline__ void visc_walk(const PassArgs<R, RN>& a, const SceneDev<R, RN>& sc, int s,
+                                          const V4<R>& p, const V4<R>& v, R& sx, R& sy, R& sz,
+                                          int& cf, int& ncand, Ranges&& ranges, Cand&& cand,
+                                          Velo&& velo) {
+    const R two_l0 = sc.two_l0, r_le = sc.r_le;
+    int* __restrict__ nb = a.nb;
+    const int nF = a.nF, K = a.nbK;
+    auto near = [&](const V4<R>& q, int j, R& d2) {
+        R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+        d2 = dot3(dx, dy, dz, dx, dy, dz);
+        return j != s && d2 <= r_le;  // dist <= r
+    };
+    auto add = [&](R d2, const V4<R>& u, int j) {
+        R d = sqrtR(d2);
+        R w = two_l0 / (d2 * d);
+        sx = fmaR(u.x - v.x, w, sx);
+        sy = fmaR(u.y - v.y, w, sy);
+        sz = fmaR(u.z - v.z, w, sz);
+        if (TAPE && cf < K) nb[size_t(cf) * nF + s] = j;
+        ++cf;
+    };
+    const V4<R> z4{R(0), R(0), R(0), R(0)};
+    // a short row's candidates are loaded together too: a batch past the row's end is
+    // padded with the particle itself, which near() rejects
+    const V4<R> self{p.x, p.y, p.z, slot_w(s, R(0))};
+    ranges([&](int lo, int hi) {
+        if (COUNT) ncand += hi - lo;
+        for (int k = lo; k < hi; k += 4) {
+            const V4<R> q0 = cand(k);
+            const V4<R> q1 = k + 1 < hi ? cand(k + 1) : self, q2 = k + 2 < hi ? cand(k + 2) : self,
+                        q3 = k + 3 < hi ? cand(k + 3) : self;
+            const int j0 = w_slot(q0.w), j1 = w_slot(q1.w), j2 = w_slot(q2.w), j3 = w_slot(q3.w);
+            R e0, e1, e2, e3;
+            const bool t0 = near(q0, j0, e0), t1 = near(q1, j1, e1), t2 = near(q2, j2, e2),
+                       t3 = near(q3, j3, e3);
+            const V4<R> u0 = t0 ? velo(k, j0) : z4, u1 = t1 ? velo(k + 1, j1) : z4,
+                        u2 = t2 ? velo(k + 2, j2) : z4, u3 = t3 ? velo(k + 3, j3) : z4;
+            if (t0) add(e0, u0, j0);
+            if (t1) add(e1, u1, j1);
+            if (t2) add(e2, u2, j2);
+            if (t3) add(e3, u3, j3);
         }
-        return;
-    }
-    const int pid = a.pid[s];
-    const SceneDev<R, RN>& sc = scene_ref(a, pid);
-    V4<R> p = ldg4(a.pos + s), v = ldg4(a.vel + s);
-    int ix, iy, iz;
-    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
-    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
-    R sx = 0, sy = 0, sz = 0;
-    int cf = 0, cm = 0;
-    {
-        // one walk over the candidates: test, then the velocity term of each neighbour in
-        // visiting order; four candidates' positions and the accepted ones' velocities in
-        // flight at a time
-        const V4<R>* __restrict__ posf = a.posf;
-        const V4<R>* __restrict__ vel = a.vel;
-        const R two_l0 = sc.two_l0, r_le = sc.r_le;
-        int* __restrict__ nb = a.nb;
-        const int nF = a.nF, K = a.nbK;
-        auto near = [&](const V4<R>& q, int j, R& d2) {
-            R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-            d2 = dot3(dx, dy, dz, dx, dy, dz);
-            return j != s && d2 <= r_le;  // dist <= r
-        };
-        auto add = [&](R d2, const V4<R>& u, int j) {
-            R d = sqrtR(d2);
-            R w = two_l0 / (d2 * d);
-            sx = fmaR(u.x - v.x, w, sx);
-            sy = fmaR(u.y - v.y, w, sy);
-            sz = fmaR(u.z - v.z, w, sz);
-            if (TAPE && cf < K) nb[size_t(cf) * nF + s] = j;
-            ++cf;
-        };
-        const V4<R> z4{R(0), R(0), R(0), R(0)};
-        // a short row's candidates are loaded together too: a batch past the row's end is
-        // padded with the particle itself, which near() rejects
-        const V4<R> self{p.x, p.y, p.z, slot_w(s, R(0))};
-        for_fluid_ranges(sc, a.csr, c, MPS_INF_SKIP(a, sc.skip_r), [&](int lo, int hi) {
-            for (int k = lo; k < hi; k += 4) {
-                const V4<R> q0 = ldg4(posf + k);
-                const V4<R> q1 = k + 1 < hi ? ldg4(posf + k + 1) : self,
-                            q2 = k + 2 < hi ? ldg4(posf + k + 2) : self,
-                            q3 = k + 3 < hi ? ldg4(posf + k + 3) : self;
-                const int j0 = w_slot(q0.w), j1 = w_slot(q1.w), j2 = w_slot(q2.w), j3 = w_slot(q3.w);
-                R e0, e1, e2, e3;
-                const bool t0 = near(q0, j0, e0), t1 = near(q1, j1, e1), t2 = near(q2, j2, e2),
-                           t3 = near(q3, j3, e3);
-                const V4<R> u0 = t0 ? ldg4(vel + j0) : z4, u1 = t1 ? ldg4(vel + j1) : z4,
-                            u2 = t2 ? ldg4(vel + j2) : z4, u3 = t3 ? ldg4(vel + j3) : z4;
-                if (t0) add(e0, u0, j0);
-                if (t1) add(e1, u1, j1);
-                if (t2) add(e2, u2, j2);
-                if (t3) add(e3, u3, j3);
-            }
-        });
-    }
+    });
+}
+
+// diagnostics: add v of every active lane of the warp to *dst with one atomic
+__device__ __forceinline__ void warp_add_u64(unsigned long long* dst, int v) {
+    const unsigned m = __activemask();
+    const unsigned tot = __reduce_add_sync(m, unsigned(v));
+    if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(dst, (unsigned long long)tot);
+}
+
+// the rest of pass A for one particle once its fluid sum is known: mirrors (VelM = 0),
+// acceleration with gravity, kick/drift (UpPcl1) and ChkPcl, the scratch outputs
+template <class R, class RN, bool DIAG, bool TAPE>
+__device__ __forceinline__ void pass_a_finish(const PassArgs<R, RN>& a, const SceneDev<R, RN>& sc,
+                                              int s, int pid, const V4<R>& p, const V4<R>& v,
+                                              const RowCtx<R>& c, R sx, R sy, R sz, int cf) {
+    int cm = 0;
     if (TAPE) a.nbcnt[s] = cf;  // the recorded list (complete while cf <= nbK)
     visc_sum_mirrors(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.m, MPS_INF_SKIP(a, sc.skip_r), sx, sy, sz,
                      cm);
@@ -668,6 +844,107 @@ __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
         d[DG_VSC_F] = cf;
         d[DG_VSC_M] = cm;
     }
+}
+
+template <class R, class RN>
+__device__ __forceinline__ void pass_a_unlisted(const PassArgs<R, RN>& a, int s, bool tape) {
+    a.tpos[s] = a.pos[s];
+    a.tvel[s] = a.vel[s];
+    a.ttyp[s] = a.typ[s];
+    if (tape) {
+        a.tape_pre[s] = V4<R>{R(0), R(0), R(0), R(kTapeDead)};
+        a.nbcnt[s] = 0;
+    }
+}
+
+// pass A: VscTrm (kernel.cu:1013-1119) + UpPcl1/ChkPcl (kernel.cu:1138-1149, 481-513), each
+// particle walking its candidates in global memory (posf through L1).
+// TAPE (recorded rollouts): also keeps the list length and the velocity before the clamp.
+template <class R, class RN, bool DIAG, bool TAPE = false>
+__global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF) return;
+    const int nalive = __ldg(a.cs + a.dead);
+    if (s >= nalive) {  // unlisted particles are carried over unchanged
+        pass_a_unlisted(a, s, TAPE);
+        return;
+    }
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    V4<R> p = ldg4(a.pos + s), v = ldg4(a.vel + s);
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    R sx = 0, sy = 0, sz = 0;
+    int cf = 0, ncand = 0;
+    const V4<R>* __restrict__ posf = a.posf;
+    const V4<R>* __restrict__ vel = a.vel;
+    visc_walk<R, RN, TAPE, DIAG>(
+        a, sc, s, p, v, sx, sy, sz, cf, ncand,
+        [&](auto&& f) { for_fluid_ranges(sc, a.csr, c, MPS_INF_SKIP(a, sc.skip_r), f); },
+        [&](int k) { return ldg4(posf + k); }, [&](int, int j) { return ldg4(vel + j); });
+    if (DIAG) warp_add_u64(&a.cnt->work[0], ncand);
+    pass_a_finish<R, RN, DIAG, TAPE>(a, sc, s, pid, p, v, c, sx, sy, sz, cf);
+}
+
+// pass A with the block's neighbourhood staged in shared memory (stage_fluid): positions,
+// and with SVEL the candidates' velocities too. Same walk order and arithmetic as k_pass_a,
+// so the results are identical; blocks whose neighbourhood does not fit walk global memory.
+template <class R, class RN, bool DIAG, bool SVEL>
+__global__ void __launch_bounds__(128) k_pass_a_st(PassArgs<R, RN> a, int cap) {
+    extern __shared__ __align__(16) unsigned char stage_mem[];
+    StageHdr& h = *reinterpret_cast<StageHdr*>(stage_mem);
+    V4<R>* spos = reinterpret_cast<V4<R>*>(stage_mem + ((sizeof(StageHdr) + 15) / 16) * 16);
+    V4<R>* svel = spos + cap;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nalive = __ldg(a.cs + a.dead);
+    const bool act = s < a.nF && s < nalive;
+    if (s < a.nF && !act) pass_a_unlisted(a, s, false);
+    int pid = 0, scene = 0;
+    V4<R> p{R(0), R(0), R(0), R(0)}, v = p;
+    RowCtx<R> c{};
+    if (act) {
+        pid = a.pid[s];
+        scene = a.nscene > 1 ? scene_of(a.sc, a.nscene, pid) : 0;
+        const SceneDev<R, RN>& sc = a.sc[scene];
+        p = ldg4(a.pos + s);
+        v = ldg4(a.vel + s);
+        int ix, iy, iz;
+        cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+        c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    }
+    auto bsel = [&](const SceneDev<R, RN>& q) { return MPS_INF_SKIP(a, q.skip_r); };
+    const bool staged = stage_fluid<R, RN, SVEL>(a, h, spos, svel, cap, act, scene, c, bsel);
+    if (DIAG && threadIdx.x == 0 && h.smax >= 0)
+        atomicAdd(staged ? &a.cnt->stage_blocks : &a.cnt->unstaged_blocks, 1);
+    if (!act) return;
+    const SceneDev<R, RN>& sc = a.sc[scene];
+    const R B = bsel(sc);
+    R sx = 0, sy = 0, sz = 0;
+    int cf = 0, ncand = 0;
+    if (staged) {
+        const V4<R>* __restrict__ vel = a.vel;
+        visc_walk<R, RN, false, DIAG>(
+            a, sc, s, p, v, sx, sy, sz, cf, ncand,
+            [&](auto&& f) {
+                for_fluid_rows(sc, c, B, [&](int fz, int fy, int xl, int xh) {
+                    int lo, hi;
+                    staged_range(h, fz, fy, xl, xh, lo, hi);
+                    f(lo, hi);
+                });
+            },
+            [&](int k) { return spos[k]; },
+            [&](int k, int j) { return SVEL ? svel[k] : ldg4(vel + j); });
+    } else {
+        const V4<R>* __restrict__ posf = a.posf;
+        const V4<R>* __restrict__ vel = a.vel;
+        visc_walk<R, RN, false, DIAG>(
+            a, sc, s, p, v, sx, sy, sz, cf, ncand,
+            [&](auto&& f) { for_fluid_ranges(sc, a.csr, c, B, f); },
+            [&](int k) { return ldg4(posf + k); }, [&](int, int j) { return ldg4(vel + j); });
+    }
+    if (DIAG) warp_add_u64(&a.cnt->work[0], ncand);
+    pass_a_finish<R, RN, DIAG, false>(a, sc, s, pid, p, v, c, sx, sy, sz, cf);
 }
 
 // pass B: ChkCol (kernel.cu:1168-1287) + MkPrs (kernel.cu:1306-1411) at x*; leaves the
@@ -691,8 +968,14 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
     R wx = v.x, wy = v.y, wz = v.z;
     RN ni = 0;
     int cnt5[5] = {0, 0, 0, 0, 0};
-    const int n = build_list(a, sc, c, s, p.x, p.y, p.z, sc.list_thr, MPS_INF_SKIP(a, sc.skip_rc));
+    int ncand = 0;
+    const int n = build_list<R, RN, DIAG>(a, sc, c, s, p.x, p.y, p.z, sc.list_thr,
+                                          MPS_INF_SKIP(a, sc.skip_rc), &ncand);
     a.nbcnt[s] = n;
+    if (DIAG) {
+        warp_add_u64(&a.cnt->work[1], ncand);
+        warp_add_u64(&a.cnt->work[2], n);
+    }
     if (n <= a.nbK) {
         const int* __restrict__ nb = a.nb + s;
         const V4<R>* __restrict__ pos = a.pos;

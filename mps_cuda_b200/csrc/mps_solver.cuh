@@ -268,6 +268,8 @@ struct SolverBase {
     bool diag_on = false, graph_on = false;
     int skip_opt = 1, block = 128;
     int grad_mode = MPS_GRAD_STANDARD;  // PrsGrdTrm variant (MPS_OPT_GRADIENT)
+    int stage_mode = MPS_STAGE_GLOBAL;  // pass A's candidate source (MPS_OPT_STAGING)
+    int stage_cap = 0;                  // candidates staged per block (MPS_OPT_STAGE_CAPACITY)
     long long steps = 0;
     long long launches = 0;       // kernels launched (graph replays included)
     long long body_launches = 0;  // kernels of one captured step
@@ -286,6 +288,7 @@ struct SolverBase {
     virtual int get_mirrors(int which, int cap, int32_t* slot, void* pos, void* prs) = 0;
     virtual void get_diag(int32_t* table, void* ndens) = 0;
     virtual void get_counters(mps_counters*) = 0;
+    virtual void get_work(mps_work*) = 0;
     virtual void integrals(int scene, double out[6]) = 0;
     virtual void invalidate_graph() = 0;
     virtual void set_list_capacity(int k) = 0;  // 0: the full capacity
@@ -766,13 +769,35 @@ template <class R, class RN> class Solver final : public SolverBase {
         invalidate_graph();
     }
 
+    // capacity of a block's stage: the option, else what keeps four blocks per SM
+    int staged_capacity() const {
+        if (stage_cap > 0) return stage_cap;
+        const bool v = stage_mode == MPS_STAGE_VELOCITIES;
+        const size_t budget = 227 * 1024 / 4 - ((sizeof(StageHdr) + 15) / 16) * 16 - 1024;
+        return int(budget / (sizeof(V4<R>) * (v ? 2 : 1)));
+    }
+    template <bool D, bool SV> void launch_pass_a_staged_v(int ba) {
+        const int cap = staged_capacity();
+        const size_t bytes = stage_smem_bytes<R>(cap, SV);
+        CK(cudaFuncSetAttribute(k_pass_a_st<R, RN, D, SV>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+        k_pass_a_st<R, RN, D, SV><<<blocks(nF, ba), ba, bytes, stream>>>(args(M1, mcs1), cap);
+    }
+    template <bool D> void launch_pass_a_staged(int ba) {
+        if (stage_mode == MPS_STAGE_VELOCITIES) launch_pass_a_staged_v<D, true>(ba);
+        else launch_pass_a_staged_v<D, false>(ba);
+    }
+
     template <bool D> void fused_body() {
         const int ba = blk[MPS_K_PASS_A], bb = blk[MPS_K_PASS_B], bc = blk[MPS_K_PASS_C],
                   bg = blk[MPS_K_GEN];
         // pass A: VscTrm + UpPcl1
         {
             Scope t(this, MPS_K_PASS_A);
-            k_pass_a<R, RN, D><<<blocks(nF, ba), ba, 0, stream>>>(args(M1, mcs1));
+            if (stage_mode == MPS_STAGE_GLOBAL)
+                k_pass_a<R, RN, D><<<blocks(nF, ba), ba, 0, stream>>>(args(M1, mcs1));
+            else
+                launch_pass_a_staged<D>(ba);
             KL();
         }
         // MkBkt on x* (kernel.cu:1917); the rebuild at kernel.cu:1921 would give the same lists
@@ -1178,6 +1203,18 @@ template <class R, class RN> class Solver final : public SolverBase {
         o->err_cell_range = c.err_cell;
         o->err_nan = c.err_nan;
         o->kernel_launches = launches;
+        o->stage_blocks = c.stage_blocks;
+        o->unstaged_blocks = c.unstaged_blocks;
+    }
+
+    void get_work(mps_work* o) override {
+        DevCounters c;
+        CK(cudaMemcpyAsync(&c, cnt, sizeof(c), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        std::memset(o, 0, sizeof(*o));
+        o->visc_candidates = (long long)c.work[0];
+        o->list_candidates = (long long)c.work[1];
+        o->list_entries = (long long)c.work[2];
     }
 
     // ---- adjoint of a recorded rollout -------------------------------------------------

@@ -82,7 +82,12 @@ struct DevCounters {
     int n_m1, n_m2;       // alive mirrors after the latest generations
     int deleted;          // particles deleted by ChkPcl (cumulative)
     int scan_ticket;      // blocks of the running fine-cell scan that finished (0 between)
-    int pad[7];
+    int stage_blocks;     // blocks of a staged pass that walked shared memory (diagnostics)
+    int unstaged_blocks;  // ... and those whose neighbourhood did not fit (diagnostics)
+    int pad[5];
+    // diagnostics: fluid candidates tested by VscTrm's walk and by the list build of
+    // ChkCol/MkPrs, and the entries of those lists
+    unsigned long long work[3];
 };
 
 }  // namespace mps

@@ -18,7 +18,7 @@ from . import _lib as L
 from ._lib import MPSError, check, lib
 
 __all__ = ["MPS", "MPSBatch", "SceneDesc", "dambreak", "dambreak_params", "derive", "select_device", "MPSError",
-           "real_dtype"]
+           "real_dtype", "measure_arith"]
 
 
 def real_dtype(precision: int):
@@ -86,6 +86,14 @@ def dambreak_params(desc: SceneDesc, snd: float = 20.0, dt: float = 2e-4, nu: fl
 def select_device(device: int) -> None:
     """Make `device` current for handles created by this thread (one process per GPU)."""
     check(lib().mps_select_device(int(device)), "mps_select_device")
+
+
+def measure_arith() -> dict:
+    """Arithmetic throughput of the current device (mps_measure_arith): FP32/FP64 fused
+    multiply-add flop/s, IEEE square roots and divisions per second, warp issue rate."""
+    a = L.mps_arith()
+    check(lib().mps_measure_arith(C.byref(a)), "mps_measure_arith")
+    return {k: getattr(a, k) for k, _ in L.mps_arith._fields_ if k != "reserved"}
 
 
 def derive(params: L.mps_params) -> L.mps_info:
@@ -237,6 +245,12 @@ class MPSBatch:
         c = L.mps_counters()
         check(lib().mps_get_counters(self._h, C.byref(c)), "mps_get_counters")
         return {k: getattr(c, k) for k, _ in L.mps_counters._fields_ if not k.startswith("reserved")}
+
+    def work(self) -> dict:
+        """Candidates tested and list entries of the steps run with MPS_OPT_DIAG."""
+        w = L.mps_work()
+        check(lib().mps_get_work(self._h, C.byref(w)), "mps_get_work")
+        return {k: getattr(w, k) for k, _ in L.mps_work._fields_ if k != "reserved"}
 
     def timing(self, reset: bool = False) -> dict:
         """Per kernel group: (total device ms, launches) of the steps timed so far."""

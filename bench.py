@@ -684,6 +684,9 @@ def measure_batched(args, stream, flush, K: int):
 
     b = MPSBatch(params, cat("typ"), f32(cat("pos")), f32(cat("vel")), f32(cat("nrm")), counts=counts)
     b.set_stream(stream.cuda_stream)
+    b.set_option(L.OPT_GRAPH, 1)
+    b.step(3)
+    ms_default = timed(lambda: b.step(1))  # default shapes: 128 threads, global walk
     tuned = b.autotune(3)
     b.set_option(L.OPT_GRAPH, 1)
     b.step(3)
@@ -708,7 +711,8 @@ def measure_batched(args, stream, flush, K: int):
             "precision": "f32 state, f64 number density", "steps": K,
             "value": nfl * K / (ms_batch / 1e3), "ms_per_step": ms_batch / K,
             "per_scene_loop_value": nfl * K / (ms_loop / 1e3), "per_scene_loop_ms_per_step": ms_loop / K,
-            "speedup_vs_per_scene_loop": ms_loop / ms_batch, "block_sizes": tuned,
+            "speedup_vs_per_scene_loop": ms_loop / ms_batch, "tuned_shapes": tuned,
+            "default_shapes_ms_per_step": ms_default / K, "tuned_gain": ms_default / ms_batch,
             "unit": "particle-updates/s"}
 
 

@@ -316,12 +316,19 @@ int mps_get_counters(mps_handle* h, mps_counters* out);
 int mps_get_timing(mps_handle* h, int32_t kernel, double* total_ms, int64_t* launches,
                    int32_t reset);
 /*
- * Autotuner: for each kernel group, time `trial_steps` steps at every candidate block size
- * (32, 64, 96, 128 threads) with CUDA events and keep the fastest. The state is restored
- * afterwards, so tuning changes no result (no kernel's arithmetic depends on its block
- * size). chosen[MPS_K_COUNT] receives the block sizes (may be NULL).
+ * Autotuner (replaces the reference's fixed THREADS 512, const.cuh:48). Each candidate is
+ * timed over `trial_steps` steps with CUDA events and the fastest kept, per kernel group:
+ * VscTrm's candidate source (MPS_OPT_STAGING: global, staged positions, staged positions
+ * and velocities) with 128 or 64 threads per block; ChkCol/MkPrs, PrsGrdTrm and the mirror
+ * generation with 128, 96, 64 or 32 threads per block. The state is restored afterwards, so
+ * tuning changes no result (no kernel's arithmetic depends on these shapes).
+ * chosen[MPS_K_COUNT] receives the block sizes (may be NULL); mps_get_option reads the
+ * staging mode. The choice is kept for the process: a handle created later with the same
+ * precision, batched or not, and fluid count in the same power-of-two class starts from it.
  */
 int mps_autotune(mps_handle* h, int32_t trial_steps, int32_t* chosen);
+/* Current value of an option (MPS_OPT_BLOCK reads VscTrm's block size). */
+int mps_get_option(mps_handle* h, int32_t opt, int32_t* value);
 /*
  * Adjoint of a rollout. The reference has no derivative of its step; these two calls add
  * one behind the same state layout.

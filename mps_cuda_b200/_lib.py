@@ -124,6 +124,7 @@ SIGNATURES = {
     "mps_get_diag": (C.c_int, [C.c_void_p, c_int32_p, C.c_void_p]),
     "mps_get_counters": (C.c_int, [C.c_void_p, C.POINTER(mps_counters)]),
     "mps_get_work": (C.c_int, [C.c_void_p, C.POINTER(mps_work)]),
+    "mps_get_option": (C.c_int, [C.c_void_p, C.c_int32, c_int32_p]),
     "mps_measure_arith": (C.c_int, [C.POINTER(mps_arith)]),
     "mps_get_timing": (C.c_int, [C.c_void_p, C.c_int32, c_double_p, C.POINTER(C.c_int64),
                                  C.c_int32]),

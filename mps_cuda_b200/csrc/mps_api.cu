@@ -9,6 +9,22 @@
 
 namespace mps {
 thread_local std::string g_last_error;
+
+namespace {
+std::mutex g_tune_mu;
+std::map<TuneKey, Tuned> g_tune;
+}  // namespace
+bool tuned_cache_get(const TuneKey& k, Tuned* out) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(k);
+    if (it == g_tune.end()) return false;
+    *out = it->second;
+    return true;
+}
+void tuned_cache_put(const TuneKey& k, const Tuned& t) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[k] = t;
+}
 }  // namespace mps
 
 // =========================================================================================
@@ -192,6 +208,24 @@ int mps_set_option(mps_handle* h, int32_t opt, int32_t value) {
                 s.grad_mode = value;
                 s.invalidate_graph();
                 break;
+            default: throw ApiError(MPS_ERR_ARG, "unknown option");
+        }
+    });
+}
+
+int mps_get_option(mps_handle* h, int32_t opt, int32_t* value) {
+    if (!value) return fail(MPS_ERR_ARG, "null value");
+    return guarded(h, [&](SolverBase& s) {
+        switch (opt) {
+            case MPS_OPT_DIAG: *value = s.diag_on; break;
+            case MPS_OPT_GRAPH: *value = s.graph_on; break;
+            case MPS_OPT_BLOCK: *value = s.blk[MPS_K_PASS_A]; break;
+            case MPS_OPT_CELL_SKIP: *value = s.skip_opt; break;
+            case MPS_OPT_TIMING: *value = s.timing_on; break;
+            case MPS_OPT_GRADIENT: *value = s.grad_mode; break;
+            case MPS_OPT_LIST_CAPACITY: *value = s.list_capacity(); break;
+            case MPS_OPT_STAGING: *value = s.stage_mode; break;
+            case MPS_OPT_STAGE_CAPACITY: *value = s.stage_cap; break;
             default: throw ApiError(MPS_ERR_ARG, "unknown option");
         }
     });

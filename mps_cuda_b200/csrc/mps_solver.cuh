@@ -12,7 +12,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -292,6 +294,7 @@ struct SolverBase {
     virtual void integrals(int scene, double out[6]) = 0;
     virtual void invalidate_graph() = 0;
     virtual void set_list_capacity(int k) = 0;  // 0: the full capacity
+    virtual int list_capacity() const = 0;
     // WrtDat's snapshot into device staging (id order, state type) and the second mirror
     // generation; the mirror count goes to pinned host memory. Then pav = 0 (kernel.cu:289).
     virtual void output_snapshot(void* pos, void* vel, void* prs, void* pav, int8_t* typ,
@@ -312,6 +315,23 @@ struct mps_handle {
 };
 
 namespace mps {
+
+// Choices of the autotuner, kept per (precision, batched, log2 of the fluid count) for the
+// life of the process: a handle created later in the same class starts from them.
+struct TuneKey {
+    int precision, batched, size_class;
+    bool operator<(const TuneKey& o) const {
+        if (precision != o.precision) return precision < o.precision;
+        if (batched != o.batched) return batched < o.batched;
+        return size_class < o.size_class;
+    }
+};
+struct Tuned {
+    int blk[MPS_K_COUNT];
+    int stage;
+};
+bool tuned_cache_get(const TuneKey& k, Tuned* out);
+void tuned_cache_put(const TuneKey& k, const Tuned& t);
 
 template <class R, class RN> class Solver final : public SolverBase {
    public:
@@ -351,7 +371,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     RN* ndens;
     IdState<R> io;
     double* d_integ;
-    int* nb;
+    uint16_t* nb16;  // the fused step's neighbour lists (16-bit entries, ListCode)
     int* nbcnt;
     int8_t* near_wall;
     static constexpr int kListCap = 160;  // about 125 neighbours lie inside r at rest density
@@ -536,6 +556,11 @@ template <class R, class RN> class Solver final : public SolverBase {
         load_fluid(false);
         mkbkt(true);
         CK(cudaStreamSynchronize(stream));
+        Tuned t;
+        if (tuned_cache_get(tune_key(), &t)) {
+            for (int k = 0; k < MPS_K_COUNT; ++k) blk[k] = t.blk[k];
+            stage_mode = t.stage;
+        }
     }
 
     void allocate() {
@@ -604,7 +629,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         io.typ = ar.template get<int8_t>(T);
         io.cell = ar.template get<int>(T);
         d_integ = ar.template get<double>(6 * size_t(nscene));
-        nb = ar.template get<int>(size_t(kListCap) * F);
+        nb16 = ar.template get<uint16_t>(size_t(kListCap) * F);
         near_wall = ar.template get<int8_t>(L());
         nbcnt = ar.template get<int>(F);
         CK(cudaMemsetAsync(S.acc, 0, sizeof(V4<R>) * F, stream));
@@ -699,7 +724,8 @@ template <class R, class RN> class Solver final : public SolverBase {
         a.m = MirrorView<R>{mcs, m.pos, m.slot};
         a.out = MirrorSink<R>{U.pos, U.slot, cap, nullptr};
         a.cnt = cnt; a.diag = diag; a.ndens = ndens;
-        a.nb = nb; a.nbcnt = nbcnt; a.nbK = nbK;
+        a.nb = nullptr;  // 32-bit lists only in recorded rollouts (tape_args)
+        a.nb16 = nb16; a.nbcnt = nbcnt; a.nbK = nbK;
         a.near_wall = near_wall;
         a.tape_pre = nullptr;
         return a;
@@ -805,7 +831,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         // pass B: ChkCol + MkPrs, then the second mirror generation at (x*, P)
         {
             Scope t(this, MPS_K_PASS_B);
-            k_pass_b<R, RN, D><<<blocks(nF, bb), bb, 0, stream>>>(args(M1, mcs1));
+            k_pass_b<R, RN, D, true><<<blocks(nF, bb), bb, 0, stream>>>(args(M1, mcs1));
             KL();
         }
         reset_raw();
@@ -822,9 +848,11 @@ template <class R, class RN> class Solver final : public SolverBase {
         {
             Scope t(this, MPS_K_PASS_C);
             if (grad_mode == MPS_GRAD_CORRECTED)
-                k_pass_c<R, RN, D, false, true><<<blocks(nF, bc), bc, 0, stream>>>(args(M2, mcs2));
+                k_pass_c<R, RN, D, false, true, true><<<blocks(nF, bc), bc, 0, stream>>>(
+                    args(M2, mcs2));
             else
-                k_pass_c<R, RN, D><<<blocks(nF, bc), bc, 0, stream>>>(args(M2, mcs2));
+                k_pass_c<R, RN, D, false, false, true><<<blocks(nF, bc), bc, 0, stream>>>(
+                    args(M2, mcs2));
             KL();
         }
         // walls that move take their place at the new time before the next step's mirrors
@@ -863,38 +891,81 @@ template <class R, class RN> class Solver final : public SolverBase {
         if (diag_on) fused_body<true>(); else fused_body<false>();
     }
 
+    // Autotuner. Candidates per kernel group, each timed over `trial` steps with CUDA events:
+    //   pass A (VscTrm): where its walk reads (global memory, staged positions, staged
+    //                    positions and velocities) x 128 or 64 threads per block;
+    //   passes B, C and mirror generation: 128, 96, 64 or 32 threads per block.
+    // All groups are timed in the same trial steps (they are separate kernels). The state is
+    // restored afterwards, and the choice is kept for later handles of the same precision
+    // and size class in this process (tuned_cache).
     void autotune(int trial, int32_t* chosen) override {
-        const int cand[] = {32, 64, 96, 128};
-        const int groups[] = {MPS_K_PASS_A, MPS_K_PASS_B, MPS_K_PASS_C, MPS_K_GEN};
+        struct CandA { int blk, stage; };
+        const CandA cand_a[] = {{128, MPS_STAGE_GLOBAL}, {64, MPS_STAGE_GLOBAL},
+                                {128, MPS_STAGE_POSITIONS}, {64, MPS_STAGE_POSITIONS},
+                                {128, MPS_STAGE_VELOCITIES}, {64, MPS_STAGE_VELOCITIES}};
+        const int cand_b[] = {128, 96, 64, 32};
+        const int groups_b[] = {MPS_K_PASS_B, MPS_K_PASS_C, MPS_K_GEN};
         double best[MPS_K_COUNT];
         int bestb[MPS_K_COUNT];
         for (int k = 0; k < MPS_K_COUNT; ++k) { best[k] = 1e300; bestb[k] = blk[k]; }
+        int best_stage = stage_mode;
         store_all();  // snapshot of the state in the id-order staging buffers
         const long long steps0 = steps;
         const bool timing0 = timing_on;
         timing_on = true;
         invalidate_graph();
         timing(0, nullptr, nullptr, true);
-        for (int b : cand) {
-            for (int g : groups) blk[g] = b;
+        const int nround = int(sizeof(cand_a) / sizeof(cand_a[0]));
+        for (int i = 0; i < nround; ++i) {
+            blk[MPS_K_PASS_A] = cand_a[i].blk;
+            stage_mode = cand_a[i].stage;
+            const bool new_b = i < 4;
+            if (new_b)
+                for (int g : groups_b) blk[g] = cand_b[i];
             step(trial);
-            for (int g : groups) {
+            auto read = [&](int g, double& ms_per) {
                 double ms = 0;
                 long long n = 0;
                 timing(g, &ms, &n, false);
-                if (n > 0 && ms / n < best[g]) { best[g] = ms / n; bestb[g] = b; }
+                ms_per = n > 0 ? ms / n : 1e300;
+            };
+            double ms;
+            read(MPS_K_PASS_A, ms);
+            if (ms < best[MPS_K_PASS_A]) {
+                best[MPS_K_PASS_A] = ms;
+                bestb[MPS_K_PASS_A] = cand_a[i].blk;
+                best_stage = cand_a[i].stage;
             }
+            if (new_b)
+                for (int g : groups_b) {
+                    read(g, ms);
+                    if (ms < best[g]) { best[g] = ms; bestb[g] = cand_b[i]; }
+                }
             timing(0, nullptr, nullptr, true);
         }
-        for (int g : groups) blk[g] = bestb[g];
+        for (int g : groups_b) blk[g] = bestb[g];
+        blk[MPS_K_PASS_A] = bestb[MPS_K_PASS_A];
+        stage_mode = best_stage;
         load_fluid(true);  // back to the snapshot: tuning leaves no trace in the results
         steps = steps0;
         timing_on = timing0;
         invalidate_graph();
         CK(cudaStreamSynchronize(stream));
+        tuned_cache_put(tune_key(), Tuned{{blk[0], blk[1], blk[2], blk[3], blk[4], blk[5]},
+                                          stage_mode});
         if (chosen)
             for (int k = 0; k < MPS_K_COUNT; ++k) chosen[k] = blk[k];
     }
+
+    // size class of the handle for the tuning cache: precision, batched or not, log2 of the
+    // fluid count
+    TuneKey tune_key() const {
+        int lg = 0;
+        while ((2LL << lg) <= (long long)std::max(nF, 1)) ++lg;
+        return TuneKey{precision, nscene > 1 ? 1 : 0, lg};
+    }
+
+    int list_capacity() const override { return nbK; }
 
     void set_list_capacity(int k) override {
         nbK = (k == 0 || k > kListCap) ? kListCap : k;
@@ -1351,7 +1422,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     void tape_prepare(const TapeStep<R>& t) {
         mkbkt(false);
         reset_raw();
-        PassArgs<R, RN> a = tape_args(M1.pos, M1.slot, mcs1, nb, nbcnt, nullptr);
+        PassArgs<R, RN> a = tape_args(M1.pos, M1.slot, mcs1, nullptr, nbcnt, nullptr);
         k_gen_cull<R, RN, false, true><<<blocks(nF, block), block, 0, stream>>>(
             a, S.pos, S.prs, S.typ);
         KL();

@@ -165,6 +165,11 @@ class MPSBatch:
     def set_stream(self, stream_ptr: int):
         check(lib().mps_set_stream(self._h, C.c_void_p(stream_ptr)), "mps_set_stream")
 
+    def get_option(self, opt: int) -> int:
+        v = C.c_int32()
+        check(lib().mps_get_option(self._h, int(opt), C.byref(v)), "mps_get_option")
+        return v.value
+
     def synchronize(self):
         check(lib().mps_synchronize(self._h), "mps_synchronize")
 
@@ -264,10 +269,13 @@ class MPSBatch:
         return out
 
     def autotune(self, trial_steps: int = 3) -> dict:
-        """Pick the fastest block size per kernel group (state restored afterwards)."""
+        """Pick the fastest shapes per kernel group (state restored afterwards): block
+        sizes, and where VscTrm's walk reads its candidates (key "staging")."""
         out = (C.c_int32 * len(L.KERNEL_GROUPS))()
         check(lib().mps_autotune(self._h, int(trial_steps), out), "mps_autotune")
-        return dict(zip(L.KERNEL_GROUPS, out[:]))
+        d = dict(zip(L.KERNEL_GROUPS, out[:]))
+        d["staging"] = self.get_option(L.OPT_STAGING)
+        return d
 
     def integrals(self, scene: int = 0) -> np.ndarray:
         out = (C.c_double * 6)()

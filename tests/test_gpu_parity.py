@@ -173,15 +173,41 @@ def test_state_roundtrip_and_errors():
     _assert_same_state(g.state(), o.state())
 
 
-def test_autotune_changes_no_result():
-    g, o, _, _ = _pair("dambreak_l0.02_6k", F32, diag=False)
+@pytest.mark.parametrize("prec", [F32, F64])
+def test_autotune_changes_no_result(prec):
+    """Tuning tries every candidate of every knob (VscTrm's staging mode and block size, the
+    other passes' block sizes) on the handle's own state and restores it: the steps after
+    it equal the oracle's. Then each knob is forced to every value it can take, and the
+    result is still the oracle's."""
+    g, o, _, _ = _pair("dambreak_l0.02_6k", prec, diag=False)
     g.step(2)
     chosen = g.autotune(2)
-    assert set(chosen["pass_a"] for _ in [0]) <= {32, 64, 96, 128}
+    assert chosen["pass_a"] in (64, 128) and chosen["staging"] in (0, 1, 2)
+    for k in ("pass_b", "pass_c", "gen_cull"):
+        assert chosen[k] in (32, 64, 96, 128)
     assert g.counters()["steps"] == 2
     g.step(3)
     o.step(5)
     _assert_same_state(g.state(), o.state())
+    g.set_option(L.OPT_GRAPH, 1)
+    for stage in (L.STAGE_GLOBAL, L.STAGE_POSITIONS, L.STAGE_VELOCITIES):
+        for blk in (32, 64, 96, 128):
+            g.set_option(L.OPT_STAGING, stage)
+            g.set_option(L.OPT_BLOCK, blk)
+            g.step(1)
+            o.step(1)
+            _assert_same_state(g.state(), o.state(), (stage, blk))
+    g.close()
+
+
+def test_tuned_shapes_carry_over_to_a_new_handle_of_the_same_class():
+    g, _, p, args = _pair("dambreak_l0.02_6k", F32, diag=False)
+    chosen = g.autotune(1)
+    h = MPS(p, *args)
+    assert h.get_option(L.OPT_STAGING) == chosen["staging"]
+    assert h.get_option(L.OPT_BLOCK) == chosen["pass_a"]
+    h.close()
+    g.close()
 
 
 def test_batch_of_64_uneven_scenes_equals_separate_handles():

@@ -691,6 +691,17 @@ def measure_batched(args, stream, flush, K: int):
     b.set_option(L.OPT_GRAPH, 1)
     b.step(3)
     ms_batch = timed(lambda: b.step(1))
+    # the kernels' own device time per step (CUDA events around each kernel group, no
+    # graph): what a persistent step could at most save is the rest
+    b.set_option(L.OPT_TIMING, 1)
+    b.timing(reset=True)
+    with torch.cuda.stream(stream):
+        for k in range(min(K, 10)):
+            flush.fill_(float(k))
+            b.step(1)
+    tm = b.timing(reset=True)
+    b.set_option(L.OPT_TIMING, 0)
+    kern_ms = sum(v[0] for v in tm.values()) / min(K, 10)
     hs = []
     for pp, pt in zip(params, parts):
         h = MPS(pp, pt["typ"], f32(pt["pos"]), f32(pt["vel"]), f32(pt["nrm"]))
@@ -713,6 +724,8 @@ def measure_batched(args, stream, flush, K: int):
             "per_scene_loop_value": nfl * K / (ms_loop / 1e3), "per_scene_loop_ms_per_step": ms_loop / K,
             "speedup_vs_per_scene_loop": ms_loop / ms_batch, "tuned_shapes": tuned,
             "default_shapes_ms_per_step": ms_default / K, "tuned_gain": ms_default / ms_batch,
+            "kernel_groups_ms_per_step": kern_ms,
+            "launch_gap_ms_per_step": ms_batch / K - kern_ms,
             "unit": "particle-updates/s"}
 
 

@@ -487,8 +487,6 @@ template <class R, class RN> struct PassArgs {
     int* nb;
     int* nbcnt;
     int nbK;
-    // the fused step's lists in 16 bits (ListCode): nb16[k * nF + s]
-    uint16_t* nb16;
     const int8_t* near_wall;  // per bucket: a wall lies in the 27 buckets around it
     // recorded rollouts only: per slot the velocity before ChkPcl's clamp, w = slot state
     // (kTapeOk, kTapeClamped, kTapeDeleted, kTapeDead)
@@ -565,76 +563,6 @@ __device__ __forceinline__ int build_list(const PassArgs<R, RN>& a, const SceneD
         }
     });
     return cnt;
-}
-
-// 16-bit list entries of the fused step. Every fluid neighbour of a particle in bucket
-// (ix, iy, iz) lies in one of the 9 bucket rows (ix-1..ix+1, iy+dy, iz+dz), each of them one
-// contiguous range of bucket-major slots starting at the slot of its first particle. An
-// entry is that row's number r = 3 dz + dy in bits 12-15 and the slot's offset from the
-// row's start in bits 0-11 (three buckets hold about a hundred particles; an offset that
-// does not fit marks the list as overflowing, and the particle walks its fine cells
-// instead, as for a long list). The row starts live in shared memory, one column per thread.
-struct ListCode {
-    int* base;  // base[r * nth + tid]: slot of the first particle of bucket row r
-    int nth, tid;
-    template <class R, class RN>
-    __device__ __forceinline__ void init(const PassArgs<R, RN>& a, const SceneDev<R, RN>& sc,
-                                         const RowCtx<R>& c) {
-#pragma unroll
-        for (int r = 0; r < 9; ++r) {
-            const int b = (c.iz - 1 + r / 3) * sc.nbxy + (c.iy - 1 + r % 3) * sc.nbx + (c.ix - 1);
-            base[r * nth + tid] = __ldg(a.cs + sc.fbase + 27 * b);
-        }
-    }
-    // the row of fine row (fz, fy) for a particle in bucket (iy, iz)
-    __device__ __forceinline__ static int row_of(int fz, int fy, int iy, int iz) {
-        return 3 * (fz / 3 - iz + 1) + (fy / 3 - iy + 1);
-    }
-    __device__ __forceinline__ int slot(unsigned e) const {
-        return base[int(e >> 12) * nth + tid] + int(e & 4095u);
-    }
-};
-
-// build_list writing 16-bit entries; returns the count, or nbK + 1 when an offset did not fit
-template <class R, class RN, bool COUNT = false>
-__device__ __forceinline__ int build_list16(const PassArgs<R, RN>& a, const SceneDev<R, RN>& sc,
-                                            const RowCtx<R>& c, const ListCode& lc, int s, R x,
-                                            R y, R z, R thr, R B, int* ncand = nullptr) {
-    int cnt = 0;
-    bool fits = true;
-    uint16_t* __restrict__ nb = a.nb16;
-    const V4<R>* __restrict__ posf = a.posf;
-    const int nF = a.nF, K = a.nbK;
-    const int nfx = 3 * sc.nbx, nfxy = 9 * sc.nbxy;
-    for_fluid_rows(sc, c, B, [&](int fz, int fy, int xl, int xh) {
-        const int row = sc.fbase + fz * nfxy + fy * nfx;
-        const int lo = __ldg(a.csr + row + xl), hi = __ldg(a.csr + row + xh + 1);
-        if (COUNT) *ncand += hi - lo;
-        const int r = ListCode::row_of(fz, fy, c.iy, c.iz);
-        const int base = lc.base[r * lc.nth + lc.tid];
-        auto visit = [&](const V4<R>& q) {
-            R dx = q.x - x, dy = q.y - y, dz = q.z - z;
-            const int j = w_slot(q.w);
-            if (j != s && dot3(dx, dy, dz, dx, dy, dz) <= thr) {
-                const unsigned off = unsigned(j - base);
-                fits = fits && off < 4096u;
-                if (cnt < K) nb[size_t(cnt) * nF + s] = uint16_t((unsigned(r) << 12) | (off & 4095u));
-                ++cnt;
-            }
-        };
-        const V4<R> self{x, y, z, slot_w(s, R(0))};
-        for (int k = lo; k < hi; k += 4) {
-            const V4<R> q0 = ldg4(posf + k);
-            const V4<R> q1 = k + 1 < hi ? ldg4(posf + k + 1) : self,
-                        q2 = k + 2 < hi ? ldg4(posf + k + 2) : self,
-                        q3 = k + 3 < hi ? ldg4(posf + k + 3) : self;
-            visit(q0);
-            visit(q1);
-            visit(q2);
-            visit(q3);
-        }
-    });
-    return fits ? cnt : max(cnt, K + 1);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1021,9 +949,8 @@ __global__ void __launch_bounds__(128) k_pass_a_st(PassArgs<R, RN> a, int cap) {
 
 // pass B: ChkCol (kernel.cu:1168-1287) + MkPrs (kernel.cu:1306-1411) at x*; leaves the
 // list of fluid neighbours inside max(rp, rlim) for pass C (same positions, same slots)
-template <class R, class RN, bool DIAG, bool L16 = false>
+template <class R, class RN, bool DIAG>
 __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
-    __shared__ int list_base[L16 ? 9 * 128 : 1];
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
     const int nalive = __ldg(a.cs + a.dead);
@@ -1042,21 +969,15 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
     RN ni = 0;
     int cnt5[5] = {0, 0, 0, 0, 0};
     int ncand = 0;
-    ListCode lc{list_base, int(blockDim.x), int(threadIdx.x)};
-    if (L16) lc.init(a, sc, c);
-    const int n = L16 ? build_list16<R, RN, DIAG>(a, sc, c, lc, s, p.x, p.y, p.z, sc.list_thr,
-                                                  MPS_INF_SKIP(a, sc.skip_rc), &ncand)
-                      : build_list<R, RN, DIAG>(a, sc, c, s, p.x, p.y, p.z, sc.list_thr,
-                                                MPS_INF_SKIP(a, sc.skip_rc), &ncand);
+    const int n = build_list<R, RN, DIAG>(a, sc, c, s, p.x, p.y, p.z, sc.list_thr,
+                                          MPS_INF_SKIP(a, sc.skip_rc), &ncand);
     a.nbcnt[s] = n;
     if (DIAG) {
         warp_add_u64(&a.cnt->work[1], ncand);
         warp_add_u64(&a.cnt->work[2], n);
     }
     if (n <= a.nbK) {
-        const int* __restrict__ nb32 = a.nb + s;
-        const uint16_t* __restrict__ nb16 = a.nb16 + s;
-        auto nb = [&](size_t e) { return L16 ? lc.slot(nb16[e]) : nb32[e]; };
+        const int* __restrict__ nb = a.nb + s;
         const V4<R>* __restrict__ pos = a.pos;
         const V4<R>* __restrict__ vel = a.vel;
         const size_t st = a.nF;
@@ -1077,8 +998,8 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
         };
         int k = 0;
         for (; k + 4 <= n; k += 4) {
-            const int j0 = nb(k * st), j1 = nb((k + 1) * st), j2 = nb((k + 2) * st),
-                      j3 = nb((k + 3) * st);
+            const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
+                      j3 = nb[(k + 3) * st];
             V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
             add(j0, q0);
             add(j1, q1);
@@ -1086,7 +1007,7 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
             add(j3, q3);
         }
         for (; k < n; ++k) {
-            const int j = nb(k * st);
+            const int j = nb[k * st];
             add(j, ldg4(pos + j));
         }
         col_dens_walls_mirrors<R, RN, true, true>(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.wl, a.m,
@@ -1118,10 +1039,9 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
 // corrected-matrix PrsGrdTrm (kernel.cu:1435-1648); where its moment matrix is all zero the
 // reference leaves in d_Acc the velocity ChkCol stored there (kernel.cu:1275, 1620), which
 // UpPcl2 then applies as the acceleration: the velocity after pass B, as here.
-template <class R, class RN, bool DIAG, bool TAPE = false, bool CORR = false, bool L16 = false>
+template <class R, class RN, bool DIAG, bool TAPE = false, bool CORR = false>
 __global__ void __launch_bounds__(128, CORR ? 6 : 8) k_pass_c(PassArgs<R, RN> a) {
     using G = typename std::conditional<CORR, GradCorr<R>, GradPlain<R>>::type;
-    __shared__ int list_base[L16 ? 9 * 128 : 1];
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
     const int nalive = __ldg(a.cs + a.dead);
@@ -1142,11 +1062,7 @@ __global__ void __launch_bounds__(128, CORR ? 6 : 8) k_pass_c(PassArgs<R, RN> a)
     int cf = 0, cm = 0;
     const int n = a.nbcnt[s];
     if (n <= a.nbK) {
-        ListCode lc{list_base, int(blockDim.x), int(threadIdx.x)};
-        if (L16) lc.init(a, sc, c);
-        const int* __restrict__ nb32 = a.nb + s;
-        const uint16_t* __restrict__ nb16 = a.nb16 + s;
-        auto nb = [&](size_t e) { return L16 ? lc.slot(nb16[e]) : nb32[e]; };
+        const int* __restrict__ nb = a.nb + s;
         const V4<R>* __restrict__ pos = a.pos;
         const R* __restrict__ prs = a.tprs;
         const size_t st = a.nF;
@@ -1161,8 +1077,8 @@ __global__ void __launch_bounds__(128, CORR ? 6 : 8) k_pass_c(PassArgs<R, RN> a)
         };
         int k = 0;
         for (; k + 4 <= n; k += 4) {
-            const int j0 = nb(k * st), j1 = nb((k + 1) * st), j2 = nb((k + 2) * st),
-                      j3 = nb((k + 3) * st);
+            const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
+                      j3 = nb[(k + 3) * st];
             V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
             const R r0 = __ldg(prs + j0), r1 = __ldg(prs + j1), r2 = __ldg(prs + j2),
                     r3 = __ldg(prs + j3);
@@ -1172,7 +1088,7 @@ __global__ void __launch_bounds__(128, CORR ? 6 : 8) k_pass_c(PassArgs<R, RN> a)
             mn(q3, r3);
         }
         for (; k < n; ++k) {
-            const int j = nb(k * st);
+            const int j = nb[k * st];
             mn(ldg4(pos + j), __ldg(prs + j));
         }
         auto gr = [&](const V4<R>& q, R pj) {
@@ -1185,8 +1101,8 @@ __global__ void __launch_bounds__(128, CORR ? 6 : 8) k_pass_c(PassArgs<R, RN> a)
             }
         };
         for (k = 0; k + 4 <= n; k += 4) {
-            const int j0 = nb(k * st), j1 = nb((k + 1) * st), j2 = nb((k + 2) * st),
-                      j3 = nb((k + 3) * st);
+            const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
+                      j3 = nb[(k + 3) * st];
             V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
             const R r0 = __ldg(prs + j0), r1 = __ldg(prs + j1), r2 = __ldg(prs + j2),
                     r3 = __ldg(prs + j3);
@@ -1196,7 +1112,7 @@ __global__ void __launch_bounds__(128, CORR ? 6 : 8) k_pass_c(PassArgs<R, RN> a)
             gr(q3, r3);
         }
         for (; k < n; ++k) {
-            const int j = nb(k * st);
+            const int j = nb[k * st];
             gr(ldg4(pos + j), __ldg(prs + j));
         }
         grad_sum_mirrors(sc, c, pid - sc.pbase, p.x, p.y, p.z, pmin, a.m, a.skip != 0, g, cm);

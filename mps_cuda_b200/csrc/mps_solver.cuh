@@ -371,7 +371,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     RN* ndens;
     IdState<R> io;
     double* d_integ;
-    uint16_t* nb16;  // the fused step's neighbour lists (16-bit entries, ListCode)
+    int* nb;
     int* nbcnt;
     int8_t* near_wall;
     static constexpr int kListCap = 160;  // about 125 neighbours lie inside r at rest density
@@ -629,7 +629,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         io.typ = ar.template get<int8_t>(T);
         io.cell = ar.template get<int>(T);
         d_integ = ar.template get<double>(6 * size_t(nscene));
-        nb16 = ar.template get<uint16_t>(size_t(kListCap) * F);
+        nb = ar.template get<int>(size_t(kListCap) * F);
         near_wall = ar.template get<int8_t>(L());
         nbcnt = ar.template get<int>(F);
         CK(cudaMemsetAsync(S.acc, 0, sizeof(V4<R>) * F, stream));
@@ -724,8 +724,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         a.m = MirrorView<R>{mcs, m.pos, m.slot};
         a.out = MirrorSink<R>{U.pos, U.slot, cap, nullptr};
         a.cnt = cnt; a.diag = diag; a.ndens = ndens;
-        a.nb = nullptr;  // 32-bit lists only in recorded rollouts (tape_args)
-        a.nb16 = nb16; a.nbcnt = nbcnt; a.nbK = nbK;
+        a.nb = nb; a.nbcnt = nbcnt; a.nbK = nbK;
         a.near_wall = near_wall;
         a.tape_pre = nullptr;
         return a;
@@ -831,7 +830,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         // pass B: ChkCol + MkPrs, then the second mirror generation at (x*, P)
         {
             Scope t(this, MPS_K_PASS_B);
-            k_pass_b<R, RN, D, true><<<blocks(nF, bb), bb, 0, stream>>>(args(M1, mcs1));
+            k_pass_b<R, RN, D><<<blocks(nF, bb), bb, 0, stream>>>(args(M1, mcs1));
             KL();
         }
         reset_raw();
@@ -848,11 +847,9 @@ template <class R, class RN> class Solver final : public SolverBase {
         {
             Scope t(this, MPS_K_PASS_C);
             if (grad_mode == MPS_GRAD_CORRECTED)
-                k_pass_c<R, RN, D, false, true, true><<<blocks(nF, bc), bc, 0, stream>>>(
-                    args(M2, mcs2));
+                k_pass_c<R, RN, D, false, true><<<blocks(nF, bc), bc, 0, stream>>>(args(M2, mcs2));
             else
-                k_pass_c<R, RN, D, false, false, true><<<blocks(nF, bc), bc, 0, stream>>>(
-                    args(M2, mcs2));
+                k_pass_c<R, RN, D><<<blocks(nF, bc), bc, 0, stream>>>(args(M2, mcs2));
             KL();
         }
         // walls that move take their place at the new time before the next step's mirrors
@@ -1422,7 +1419,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     void tape_prepare(const TapeStep<R>& t) {
         mkbkt(false);
         reset_raw();
-        PassArgs<R, RN> a = tape_args(M1.pos, M1.slot, mcs1, nullptr, nbcnt, nullptr);
+        PassArgs<R, RN> a = tape_args(M1.pos, M1.slot, mcs1, nb, nbcnt, nullptr);
         k_gen_cull<R, RN, false, true><<<blocks(nF, block), block, 0, stream>>>(
             a, S.pos, S.prs, S.typ);
         KL();

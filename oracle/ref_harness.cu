@@ -225,6 +225,29 @@ int ref_get_buckets(void* h, int* cell_of) {
     return visited;
 }
 
+// the particles of every bucket in the order of the reference's linked lists (bfst / nxt):
+// order[start[b] .. start[b+1]) for bucket b; start has nBxyz + 1 entries. Returns the number
+// of entries written (at most cap).
+int ref_get_list_order(void* h, int cap, int* order, int* start) {
+    MPS* o = static_cast<MPS*>(h);
+    const int n = o->nP, nb = o->nBxyz;
+    std::vector<int> bfst(nb), nxt(n);
+    cudaMemcpy(bfst.data(), o->d_bfst, sizeof(int) * nb, cudaMemcpyDeviceToHost);
+    cudaMemcpy(nxt.data(), o->d_nxt, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    int at = 0;
+    for (int b = 0; b < nb; ++b) {
+        start[b] = at;
+        int j = bfst[b], guard = 0;
+        while (j >= 0 && j < n && guard++ <= n) {
+            if (at < cap) order[at] = j;
+            ++at;
+            j = nxt[j];
+        }
+    }
+    start[nb] = at;
+    return at;
+}
+
 // derived constants: n0, lmd, n0_grad, lmd_grad, Numn0_grad, r, rp, DB, DBinv, nBx, nBy, nBz,
 // rlim2, COL, Prs_coef, MINc xyz, MAXc xyz
 int ref_get_info(void* h, double* out) {

@@ -47,6 +47,7 @@ def lib(precision: int, corrected: bool = False):
         L.ref_get_wall_flags.argtypes = [C.c_void_p, c_int8_p]
         L.ref_get_mirrors.argtypes = [C.c_void_p, c_int8_p, C.c_void_p, C.c_void_p, c_int32_p]
         L.ref_get_buckets.argtypes = [C.c_void_p, c_int32_p]
+        L.ref_get_list_order.argtypes = [C.c_void_p, C.c_int, c_int32_p, c_int32_p]
         L.ref_get_info.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         _libs[key] = L
     return _libs[key]
@@ -116,6 +117,16 @@ class Reference:
         o = np.empty(self.n, np.int32)
         self.L.ref_get_buckets(self.h, o.ctypes.data_as(c_int32_p))
         return o
+
+    def list_order(self):
+        """Per bucket, the particles in the order of the reference's linked lists:
+        (order, start) with bucket b's particles order[start[b]:start[b + 1]]."""
+        nb = int(self.info()["nbx"] * self.info()["nby"] * self.info()["nbz"])
+        order = np.empty(self.n, np.int32)
+        start = np.empty(nb + 1, np.int32)
+        self.L.ref_get_list_order(self.h, self.n, order.ctypes.data_as(c_int32_p),
+                                  start.ctypes.data_as(c_int32_p))
+        return order, start
 
     def info(self):
         v = (C.c_double * 21)()

@@ -38,7 +38,9 @@ def test_work_counts_bound_the_pairs_and_ignore_staging():
             g.step(1)
             w, d = g.work(), g.diag()
             fluid = int((g.state()["typ"] == 0).sum())
-            assert w["visc_candidates"] >= int(d["vsc_f"].sum()) > 100 * fluid
+            # about 100 neighbours inside r per particle at rest density (fewer at the walls
+            # and the free surface), about twice as many candidates tested
+            assert w["visc_candidates"] >= int(d["vsc_f"].sum()) > 50 * fluid
             assert w["list_candidates"] >= w["list_entries"] >= int(d["prs_f"].sum())
             assert w["list_entries"] >= int(d["col_f"].sum())
             seen.append(w)

@@ -139,13 +139,7 @@ __device__ __forceinline__ int fine_rowmajor(const SceneDev<R, RN>& sc, int c) {
     return sc.fbase + fz * (9 * sc.nbxy) + fy * (3 * sc.nbx) + fx;
 }
 
-// Visit the fluid of the 27 buckets around c in fine cells, z, y, x ascending, ascending
-// particle id inside a fine cell, through the row-ordered copy posf (start table csr):
-// f(slot, position) for every particle of the cells within sqrt(B) of the particle. `B` is
-// (radius + margin)^2, the margin (1e-3 of a bucket) covering the float geometry. The
-// neighbours inside the radius, and their order, are those of a walk over every fine cell
-// of the 27 buckets.
-// The fine rows of that walk: g(fz, fy, xl, xh) for every fine row (fz, fy) within sqrt(B),
+// The fine rows of the fluid walk below: g(fz, fy, xl, xh) for every fine row (fz, fy) within sqrt(B),
 // z then y ascending, with the fine cells [xl, xh] of the row it reaches. Every step is
 // monotone in the particle's coordinates (IEEE arithmetic, clamps, truncation), which the
 // staged walk relies on to bound the rows of a whole block from the box around its
@@ -169,6 +163,12 @@ __device__ __forceinline__ void for_fluid_rows(const SceneDev<R, RN>& sc, const 
     }
 }
 
+// Visit the fluid of the 27 buckets around c in fine cells, z, y, x ascending, ascending
+// particle id inside a fine cell, through the row-ordered copy posf (start table csr):
+// f(lo, hi) for the range of posf of every fine row's cells within sqrt(B) of the particle.
+// `B` is (radius + margin)^2, the margin (1e-3 of a bucket) covering the float geometry. The
+// neighbours inside the radius, and their order, are those of a walk over every fine cell
+// of the 27 buckets.
 template <class R, class RN, class F>
 __device__ __forceinline__ void for_fluid_ranges(const SceneDev<R, RN>& sc,
                                                  const int* __restrict__ csr, const RowCtx<R>& c,
@@ -640,13 +640,33 @@ __device__ __forceinline__ int plan_mirrors(const SceneDev<R, RN>& sc, const Row
     });
     pl.nreg = reg.n;
     pl.corner = -1;
-    // corner mirror through the last Edge wall (kernel.cu:841-858)
+    // corner mirror through an Edge wall with the last registered Edge normal
+    // (kernel.cu:841-858). The reference takes the first such wall its lists hold; with two
+    // Edge normals (next to one edge of the tank) the nearest one is taken canonically, the
+    // first found among equally near ones: it lies on that edge, the plane the reference's
+    // runs pick there. Next to a vertex (three normals) the first one found stays.
     if (reg.n > 0 && edge.n >= 2) {
         R sx, sy, sz;
         edge.sum(sx, sy, sz);
         R as = sqrtR(dot3(sx, sy, sz, sx, sy, sz));
         pl.sx = sx / as; pl.sy = sy / as; pl.sz = sz / as;
         pl.corner = last_edge;
+        if (edge.n == 2) {
+            const V4<R> ln = ldg4(wl.nrm + last_edge);
+            R best = R(INFINITY);
+            for_rows(sc, wl.cs, c, skip ? sc.skip_r : R(INFINITY), [&](int j) {
+                if (__ldg(wl.wse + j) != kEDGE) return;
+                const V4<R> nv = ldg4(wl.nrm + j);
+                if (nv.x != ln.x || nv.y != ln.y || nv.z != ln.z) return;
+                const V4<R> q = ldg4(wl.pos + j);
+                const R dx = x - q.x, dy = y - q.y, dz = z - q.z;
+                const R d2 = dot3(dx, dy, dz, dx, dy, dz);
+                if (d2 <= sc.r2 && d2 < best) {
+                    best = d2;
+                    pl.corner = j;
+                }
+            });
+        }
     }
     return nwall;
 }

@@ -29,6 +29,11 @@
 //     The candidates are the reference's (the particles of the 27 buckets); only the
 //     order of the sums is fixed this way;
 //   * ChkCol visits fluid neighbours, then wall neighbours, then mirrors;
+//   * with two distinct Edge normals in reach, the corner mirror's plane point is the
+//     NEAREST Edge wall with the last registered Edge normal, where the reference takes the
+//     first one its lists hold (kernel.cu:852-858): near a tank edge that is a wall on the
+//     edge itself, the plane the reference's runs choose there, while the first wall in id
+//     order can lie on another border of the face;
 //   * arithmetic is written with explicit fma where a product feeds a sum (the forms an
 //     FMA-contracting compiler produces) and is built with -ffp-contract=off, so every
 //     expression rounds the same way on every machine;
@@ -428,6 +433,24 @@ struct Oracle {
             }
             // corner mirror from the normalised sum of edge normals (:841-887)
             if (nedge >= 2) {
+                // Its plane point: an Edge wall with the last registered Edge normal. The
+                // reference takes the first such wall its linked lists happen to hold
+                // (:852-858), an order that changes with thread scheduling. With two Edge
+                // normals (a particle next to one edge of the tank) the nearest such wall is
+                // taken canonically (the first found among equally near ones): it lies on
+                // that edge, the plane the reference's runs pick there. Next to a vertex
+                // (three normals) the first one in visiting order stays.
+                const int wl = edgeu[nedge - 1];
+                int best = wl;
+                R best_d2 = R(INFINITY);
+                if (nedge == 2) for_nb(cstart, clist, ix, iy, iz, [&](int j) {
+                    if (!is_wall(typ[j]) || wse[j] != EDGE) return;
+                    if (nx[j] != nx[wl] || ny[j] != ny[wl] || nz[j] != nz[wl]) return;
+                    R qx = x - px[j], qy = y - py[j], qz = z - pz[j];
+                    R d2 = dot3(qx, qy, qz, qx, qy, qz);
+                    if (d2 <= r2 && d2 < best_d2) { best_d2 = d2; best = j; }
+                });
+                edgeu[nedge - 1] = best;
                 R sx = 0, sy = 0, sz = 0, pwx = 0, pwy = 0, pwz = 0, wx = 0, wy = 0, wz = 0;
                 for (int k = 0; k < nedge; ++k) {
                     int w = edgeu[k];

@@ -365,6 +365,9 @@ def run_ours(args, world, rank, local):
     g = MPS(p, typ, pos, vel, nrm)
     stream = torch.cuda.Stream()
     g.set_stream(stream.cuda_stream)
+    # the library's tuned shapes for this scene (mps_autotune restores the state it tried
+    # them on), as a user calls it once per handle
+    tuned = None if args.no_tune else g.autotune(3)
     g.set_option(L.OPT_GRAPH, 1)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
@@ -512,7 +515,7 @@ def run_ours(args, world, rank, local):
             "dtype": args.precision, "data": "synthetic",
             "config": bench_config(args.workload, args.precision, nf, int((typ != 0).sum()),
                                    world),
-            "graph": True,
+            "graph": True, "tuned_shapes": tuned,
             "clocks": clk.summary(), "wall_ms_per_step": 1e3 * wall / K,
             "e2e": e2e, "gpu_launches": launches,
             "roofline": roofline, "compute_roofline": compute, "kernel_groups": groups,
@@ -743,6 +746,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--no-compute", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
     args = ap.parse_args()
     world, rank, local = setup_dist()
     try:

@@ -160,9 +160,11 @@ enum {
                                 instead, with the same result; lower values exercise that
                                 path. Changing it voids a recorded adjoint rollout.       */
     MPS_OPT_STAGING = 7,     /* where VscTrm's candidate walk reads: MPS_STAGE_*         */
-    MPS_OPT_STAGE_CAPACITY = 8 /* candidates a block may stage in shared memory (0 = the
+    MPS_OPT_STAGE_CAPACITY = 8, /* candidates a block may stage in shared memory (0 = the
                                 default); a block whose neighbourhood holds more walks
                                 global memory. Results never depend on it.               */
+    MPS_OPT_CANDIDATE_BATCH = 9 /* VscTrm's candidates loaded together per particle: 2, 4
+                                or 8 (0 = 4). Results never depend on it.                */
 };
 
 /* MPS_OPT_STAGING. GLOBAL: each particle walks its fine cells through L1. POSITIONS: a block
@@ -318,8 +320,8 @@ int mps_get_timing(mps_handle* h, int32_t kernel, double* total_ms, int64_t* lau
 /*
  * Autotuner (replaces the reference's fixed THREADS 512, const.cuh:48). Each candidate is
  * timed over `trial_steps` steps with CUDA events and the fastest kept, per kernel group:
- * VscTrm's candidate source (MPS_OPT_STAGING: global, staged positions, staged positions
- * and velocities) with 128 or 64 threads per block; ChkCol/MkPrs, PrsGrdTrm and the mirror
+ * VscTrm's candidates in flight (MPS_OPT_CANDIDATE_BATCH: 2, 4, 8), threads per block (128,
+ * 64) and candidate source (MPS_OPT_STAGING); ChkCol/MkPrs, PrsGrdTrm and the mirror
  * generation with 128, 96, 64 or 32 threads per block. The state is restored afterwards, so
  * tuning changes no result (no kernel's arithmetic depends on these shapes).
  * chosen[MPS_K_COUNT] receives the block sizes (may be NULL); mps_get_option reads the

@@ -29,6 +29,10 @@ WORKLOADS = {
     # 160x160x240 = 6144000 fluid particles, l0 = 0.0025, 1.6 x 0.4 x 0.8 tank
     "dambreak_l0.0025_6.1M": (SceneDesc(0.0025, (1.6, 0.4, 0.8), (160, 160, 240), seed=0), 2.5e-5,
                               500),
+    # 125x125x187 = 2921875 fluid particles, l0 = 0.0032: a state larger than L2 that a
+    # profiler capture can hold (the 6.1M scene's traffic scaled down)
+    "dambreak_l0.0032_2.9M": (SceneDesc(0.0032, (1.6, 0.4, 0.8), (125, 125, 187), seed=0), 3.2e-5,
+                              500),
     # small scene for golden vectors and quick checks
     "dambreak_l0.02_small": (SceneDesc(0.02, (0.4, 0.2, 0.4), (8, 6, 10), seed=3), 2e-4, 50),
 }

@@ -196,6 +196,12 @@ int mps_set_option(mps_handle* h, int32_t opt, int32_t value) {
                 s.stage_mode = value;
                 s.invalidate_graph();
                 break;
+            case MPS_OPT_CANDIDATE_BATCH:
+                if (value != 0 && value != 2 && value != 4 && value != 8)
+                    throw ApiError(MPS_ERR_ARG, "candidate batch must be 0, 2, 4 or 8");
+                s.batch_a = value ? value : 4;
+                s.invalidate_graph();
+                break;
             case MPS_OPT_STAGE_CAPACITY:
                 if (value < 0 || value > (1 << 16))
                     throw ApiError(MPS_ERR_ARG, "stage capacity must lie in [0, 65536]");
@@ -226,6 +232,7 @@ int mps_get_option(mps_handle* h, int32_t opt, int32_t* value) {
             case MPS_OPT_LIST_CAPACITY: *value = s.list_capacity(); break;
             case MPS_OPT_STAGING: *value = s.stage_mode; break;
             case MPS_OPT_STAGE_CAPACITY: *value = s.stage_cap; break;
+            case MPS_OPT_CANDIDATE_BATCH: *value = s.batch_a; break;
             default: throw ApiError(MPS_ERR_ARG, "unknown option");
         }
     });

@@ -760,11 +760,13 @@ __device__ __forceinline__ void tape_record(const PassArgs<R, RN>& a, const Scen
 }
 
 // Pass A's candidate walk for one particle: each candidate tested, then the velocity term of
-// each neighbour in visiting order; four candidates' positions and the accepted ones'
-// velocities in flight at a time. ranges(f) hands the candidate ranges [lo, hi) to f in
-// visiting order; cand(k) is candidate k's position (w = slot), velo(k, j) the velocity of
-// candidate k (slot j). TAPE: the neighbours' slots also go to the slot's list.
-template <class R, class RN, bool TAPE, bool COUNT, class Ranges, class Cand, class Velo>
+// each neighbour in visiting order; NB candidates' positions and the accepted ones'
+// velocities in flight at a time (NB = 2, 4 or 8, MPS_OPT_CANDIDATE_BATCH). ranges(f) hands
+// the candidate ranges [lo, hi) to f in visiting order; cand(k) is candidate k's position
+// (w = slot), velo(k, j) the velocity of candidate k (slot j). TAPE: the neighbours' slots
+// also go to the slot's list.
+template <class R, class RN, bool TAPE, bool COUNT, int NB = 4, class Ranges, class Cand,
+          class Velo>
 __device__ __forceinline__ void visc_walk(const PassArgs<R, RN>& a, const SceneDev<R, RN>& sc, int s,
                                           const V4<R>& p, const V4<R>& v, R& sx, R& sy, R& sz,
                                           int& cf, int& ncand, Ranges&& ranges, Cand&& cand,
@@ -792,20 +794,25 @@ __device__ __forceinline__ void visc_walk(const PassArgs<R, RN>& a, const SceneD
     const V4<R> self{p.x, p.y, p.z, slot_w(s, R(0))};
     ranges([&](int lo, int hi) {
         if (COUNT) ncand += hi - lo;
-        for (int k = lo; k < hi; k += 4) {
-            const V4<R> q0 = cand(k);
-            const V4<R> q1 = k + 1 < hi ? cand(k + 1) : self, q2 = k + 2 < hi ? cand(k + 2) : self,
-                        q3 = k + 3 < hi ? cand(k + 3) : self;
-            const int j0 = w_slot(q0.w), j1 = w_slot(q1.w), j2 = w_slot(q2.w), j3 = w_slot(q3.w);
-            R e0, e1, e2, e3;
-            const bool t0 = near(q0, j0, e0), t1 = near(q1, j1, e1), t2 = near(q2, j2, e2),
-                       t3 = near(q3, j3, e3);
-            const V4<R> u0 = t0 ? velo(k, j0) : z4, u1 = t1 ? velo(k + 1, j1) : z4,
-                        u2 = t2 ? velo(k + 2, j2) : z4, u3 = t3 ? velo(k + 3, j3) : z4;
-            if (t0) add(e0, u0, j0);
-            if (t1) add(e1, u1, j1);
-            if (t2) add(e2, u2, j2);
-            if (t3) add(e3, u3, j3);
+        for (int k = lo; k < hi; k += NB) {
+            V4<R> q[NB];
+            q[0] = cand(k);
+#pragma unroll
+            for (int t = 1; t < NB; ++t) q[t] = k + t < hi ? cand(k + t) : self;
+            int j[NB];
+            R e[NB];
+            bool ok[NB];
+#pragma unroll
+            for (int t = 0; t < NB; ++t) {
+                j[t] = w_slot(q[t].w);
+                ok[t] = near(q[t], j[t], e[t]);
+            }
+            V4<R> u[NB];
+#pragma unroll
+            for (int t = 0; t < NB; ++t) u[t] = ok[t] ? velo(k + t, j[t]) : z4;
+#pragma unroll
+            for (int t = 0; t < NB; ++t)
+                if (ok[t]) add(e[t], u[t], j[t]);
         }
     });
 }
@@ -860,7 +867,7 @@ __device__ __forceinline__ void pass_a_unlisted(const PassArgs<R, RN>& a, int s,
 // pass A: VscTrm (kernel.cu:1013-1119) + UpPcl1/ChkPcl (kernel.cu:1138-1149, 481-513), each
 // particle walking its candidates in global memory (posf through L1).
 // TAPE (recorded rollouts): also keeps the list length and the velocity before the clamp.
-template <class R, class RN, bool DIAG, bool TAPE = false>
+template <class R, class RN, bool DIAG, bool TAPE = false, int NB = 4>
 __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
@@ -879,7 +886,7 @@ __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
     int cf = 0, ncand = 0;
     const V4<R>* __restrict__ posf = a.posf;
     const V4<R>* __restrict__ vel = a.vel;
-    visc_walk<R, RN, TAPE, DIAG>(
+    visc_walk<R, RN, TAPE, DIAG, NB>(
         a, sc, s, p, v, sx, sy, sz, cf, ncand,
         [&](auto&& f) { for_fluid_ranges(sc, a.csr, c, MPS_INF_SKIP(a, sc.skip_r), f); },
         [&](int k) { return ldg4(posf + k); }, [&](int, int j) { return ldg4(vel + j); });

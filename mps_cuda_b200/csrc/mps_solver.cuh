@@ -272,6 +272,7 @@ struct SolverBase {
     int grad_mode = MPS_GRAD_STANDARD;  // PrsGrdTrm variant (MPS_OPT_GRADIENT)
     int stage_mode = MPS_STAGE_GLOBAL;  // pass A's candidate source (MPS_OPT_STAGING)
     int stage_cap = 0;                  // candidates staged per block (MPS_OPT_STAGE_CAPACITY)
+    int batch_a = 4;                    // VscTrm's candidates in flight (MPS_OPT_CANDIDATE_BATCH)
     long long steps = 0;
     long long launches = 0;       // kernels launched (graph replays included)
     long long body_launches = 0;  // kernels of one captured step
@@ -328,7 +329,7 @@ struct TuneKey {
 };
 struct Tuned {
     int blk[MPS_K_COUNT];
-    int stage;
+    int stage, batch;
 };
 bool tuned_cache_get(const TuneKey& k, Tuned* out);
 void tuned_cache_put(const TuneKey& k, const Tuned& t);
@@ -560,6 +561,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         if (tuned_cache_get(tune_key(), &t)) {
             for (int k = 0; k < MPS_K_COUNT; ++k) blk[k] = t.blk[k];
             stage_mode = t.stage;
+            batch_a = t.batch;
         }
     }
 
@@ -819,7 +821,11 @@ template <class R, class RN> class Solver final : public SolverBase {
         // pass A: VscTrm + UpPcl1
         {
             Scope t(this, MPS_K_PASS_A);
-            if (stage_mode == MPS_STAGE_GLOBAL)
+            if (stage_mode == MPS_STAGE_GLOBAL && batch_a == 2)
+                k_pass_a<R, RN, D, false, 2><<<blocks(nF, ba), ba, 0, stream>>>(args(M1, mcs1));
+            else if (stage_mode == MPS_STAGE_GLOBAL && batch_a == 8)
+                k_pass_a<R, RN, D, false, 8><<<blocks(nF, ba), ba, 0, stream>>>(args(M1, mcs1));
+            else if (stage_mode == MPS_STAGE_GLOBAL)
                 k_pass_a<R, RN, D><<<blocks(nF, ba), ba, 0, stream>>>(args(M1, mcs1));
             else
                 launch_pass_a_staged<D>(ba);
@@ -889,23 +895,23 @@ template <class R, class RN> class Solver final : public SolverBase {
     }
 
     // Autotuner. Candidates per kernel group, each timed over `trial` steps with CUDA events:
-    //   pass A (VscTrm): where its walk reads (global memory, staged positions, staged
-    //                    positions and velocities) x 128 or 64 threads per block;
+    //   pass A (VscTrm): candidates in flight (2, 4, 8) and 128 or 64 threads per block
+    //                    for the walk through L1, and the staged walk at 128 threads;
     //   passes B, C and mirror generation: 128, 96, 64 or 32 threads per block.
     // All groups are timed in the same trial steps (they are separate kernels). The state is
     // restored afterwards, and the choice is kept for later handles of the same precision
     // and size class in this process (tuned_cache).
     void autotune(int trial, int32_t* chosen) override {
-        struct CandA { int blk, stage; };
-        const CandA cand_a[] = {{128, MPS_STAGE_GLOBAL}, {64, MPS_STAGE_GLOBAL},
-                                {128, MPS_STAGE_POSITIONS}, {64, MPS_STAGE_POSITIONS},
-                                {128, MPS_STAGE_VELOCITIES}, {64, MPS_STAGE_VELOCITIES}};
+        struct CandA { int blk, stage, batch; };
+        const CandA cand_a[] = {{128, MPS_STAGE_GLOBAL, 4}, {64, MPS_STAGE_GLOBAL, 4},
+                                {128, MPS_STAGE_GLOBAL, 2}, {64, MPS_STAGE_GLOBAL, 2},
+                                {128, MPS_STAGE_GLOBAL, 8}, {128, MPS_STAGE_POSITIONS, 4}};
         const int cand_b[] = {128, 96, 64, 32};
         const int groups_b[] = {MPS_K_PASS_B, MPS_K_PASS_C, MPS_K_GEN};
         double best[MPS_K_COUNT];
         int bestb[MPS_K_COUNT];
         for (int k = 0; k < MPS_K_COUNT; ++k) { best[k] = 1e300; bestb[k] = blk[k]; }
-        int best_stage = stage_mode;
+        int best_stage = stage_mode, best_batch = batch_a;
         store_all();  // snapshot of the state in the id-order staging buffers
         const long long steps0 = steps;
         const bool timing0 = timing_on;
@@ -916,6 +922,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         for (int i = 0; i < nround; ++i) {
             blk[MPS_K_PASS_A] = cand_a[i].blk;
             stage_mode = cand_a[i].stage;
+            batch_a = cand_a[i].batch;
             const bool new_b = i < 4;
             if (new_b)
                 for (int g : groups_b) blk[g] = cand_b[i];
@@ -932,6 +939,7 @@ template <class R, class RN> class Solver final : public SolverBase {
                 best[MPS_K_PASS_A] = ms;
                 bestb[MPS_K_PASS_A] = cand_a[i].blk;
                 best_stage = cand_a[i].stage;
+                best_batch = cand_a[i].batch;
             }
             if (new_b)
                 for (int g : groups_b) {
@@ -943,13 +951,14 @@ template <class R, class RN> class Solver final : public SolverBase {
         for (int g : groups_b) blk[g] = bestb[g];
         blk[MPS_K_PASS_A] = bestb[MPS_K_PASS_A];
         stage_mode = best_stage;
+        batch_a = best_batch;
         load_fluid(true);  // back to the snapshot: tuning leaves no trace in the results
         steps = steps0;
         timing_on = timing0;
         invalidate_graph();
         CK(cudaStreamSynchronize(stream));
         tuned_cache_put(tune_key(), Tuned{{blk[0], blk[1], blk[2], blk[3], blk[4], blk[5]},
-                                          stage_mode});
+                                          stage_mode, batch_a});
         if (chosen)
             for (int k = 0; k < MPS_K_COUNT; ++k) chosen[k] = blk[k];
     }

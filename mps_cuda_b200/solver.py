@@ -275,6 +275,7 @@ class MPSBatch:
         check(lib().mps_autotune(self._h, int(trial_steps), out), "mps_autotune")
         d = dict(zip(L.KERNEL_GROUPS, out[:]))
         d["staging"] = self.get_option(L.OPT_STAGING)
+        d["candidate_batch"] = self.get_option(L.OPT_CANDIDATE_BATCH)
         return d
 
     def integrals(self, scene: int = 0) -> np.ndarray:

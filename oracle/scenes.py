@@ -54,6 +54,7 @@ WORKLOADS = {
     "adjoint_l0.01_48k": (Scene(0.01, (1.0, 0.2, 0.8), (40, 20, 60), vel_sigma=0.05, vel_seed=1),
                           1e-4, 200),
     "dambreak_l0.0025_6.1M": (Scene(0.0025, (1.6, 0.4, 0.8), (160, 160, 240)), 2.5e-5, 500),
+    "dambreak_l0.0032_2.9M": (Scene(0.0032, (1.6, 0.4, 0.8), (125, 125, 187)), 3.2e-5, 500),
     "dambreak_l0.02_small": (Scene(0.02, (0.4, 0.2, 0.4), (8, 6, 10), seed=3), 2e-4, 50),
 }
 

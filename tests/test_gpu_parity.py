@@ -183,6 +183,7 @@ def test_autotune_changes_no_result(prec):
     g.step(2)
     chosen = g.autotune(2)
     assert chosen["pass_a"] in (64, 128) and chosen["staging"] in (0, 1, 2)
+    assert chosen["candidate_batch"] in (2, 4, 8)
     for k in ("pass_b", "pass_c", "gen_cull"):
         assert chosen[k] in (32, 64, 96, 128)
     assert g.counters()["steps"] == 2
@@ -197,6 +198,12 @@ def test_autotune_changes_no_result(prec):
             g.step(1)
             o.step(1)
             _assert_same_state(g.state(), o.state(), (stage, blk))
+    g.set_option(L.OPT_STAGING, L.STAGE_GLOBAL)
+    for nb in (2, 8, 4):
+        g.set_option(L.OPT_CANDIDATE_BATCH, nb)
+        g.step(1)
+        o.step(1)
+        _assert_same_state(g.state(), o.state(), ("batch", nb))
     g.close()
 
 

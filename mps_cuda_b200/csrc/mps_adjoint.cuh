@@ -112,7 +112,7 @@ template <class R, class RN> __global__ void __launch_bounds__(128) k_adj_c1(Adj
             const V4<R> p = a.t.x2[s];
             pm = a.t.P2[s];
             for (int k = 0; k < n; ++k) {
-                const int j = a.t.nbB[size_t(k) * a.nF + s];
+                const int j = a.t.nbB[list_at(s, k, a.nbK)];
                 const V4<R> q = ldg4(a.t.x2 + j);
                 R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
                 if (dot3(dx, dy, dz, dx, dy, dz) < sc.rp2) {
@@ -162,7 +162,7 @@ template <class R, class RN> __global__ void __launch_bounds__(128) k_adj_c2(Adj
     D3 accx = d3d(a.lxs[s]), sphi = d3(0, 0, 0);
     double accP = 0.0;
     for (int k = 0; k < n; ++k) {
-        const int i = a.t.nbB[size_t(k) * a.nF + s];
+        const int i = a.t.nbB[list_at(s, k, a.nbK)];
         const V4<R> q = ldg4(a.t.x2 + i);
         R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
         if (!(dot3(dx, dy, dz, dx, dy, dz) < sc.rp2)) continue;
@@ -242,7 +242,7 @@ template <class R, class RN> __global__ void __launch_bounds__(128) k_adj_b2(Adj
     const double lns = adj_ln(a, sc, s), rp = double(sc.rp), colfac = double(sc.colfac);
     D3 accx = d3d(a.lxs[s]) + d3d(a.lx_at[s]), accu = lvs;
     for (int k = 0; k < n; ++k) {
-        const int i = a.t.nbB[size_t(k) * a.nF + s];
+        const int i = a.t.nbB[list_at(s, k, a.nbK)];
         const V4<R> q = ldg4(a.t.x2 + i);
         R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
         const R d2r = dot3(dx, dy, dz, dx, dy, dz);
@@ -337,7 +337,7 @@ template <class R, class RN> __global__ void __launch_bounds__(128) k_adj_a2(Adj
             const D3 lSs = kn * las;
             D3 accx = d3d(a.lxa[s]), accv = d3d(a.lva[s]), S = d3(0, 0, 0);
             for (int k = 0; k < n; ++k) {
-                const int i = a.t.nbA[size_t(k) * a.nF + s];
+                const int i = a.t.nbA[list_at(s, k, a.nbK)];
                 const D3 r = d3v(ldg4(a.t.x1 + i)) - x;
                 const D3 vi = d3v(ldg4(a.t.v1 + i));
                 const double d2 = dot(r, r), d = sqrt(d2), w = two_l0 / (d2 * d);

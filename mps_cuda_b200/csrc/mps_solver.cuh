@@ -631,7 +631,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         io.typ = ar.template get<int8_t>(T);
         io.cell = ar.template get<int>(T);
         d_integ = ar.template get<double>(6 * size_t(nscene));
-        nb = ar.template get<int>(size_t(kListCap) * F);
+        nb = ar.template get<int>(size_t(kListCap) * ((F + 31) / 32 * 32));  // list_at tiles
         near_wall = ar.template get<int8_t>(L());
         nbcnt = ar.template get<int>(F);
         CK(cudaMemsetAsync(S.acc, 0, sizeof(V4<R>) * F, stream));
@@ -1345,6 +1345,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         st->nbK = nbK;
         DevArena& a = st->ar;
         const size_t F = std::max(nF, 1), T = std::max(nT, 1), Cm = size_t(cap), Lc = L() + 1;
+        const size_t F32 = (F + 31) / 32 * 32;  // slots rounded to whole warps (list_at)
         for (int c = 0; c <= nck; ++c)
             st->ck.push_back(Ckpt{a.template get<R>(3 * T), a.template get<R>(3 * T),
                                   a.template get<R>(T), a.template get<R>(T),
@@ -1353,13 +1354,13 @@ template <class R, class RN> class Solver final : public SolverBase {
             TapeStep<R> t;
             t.pid1 = a.template get<int>(F); t.x1 = a.template get<V4<R>>(F);
             t.v1 = a.template get<V4<R>>(F); t.up1 = a.template get<V4<R>>(F);
-            t.nA = a.template get<int>(F); t.nbA = a.template get<int>(size_t(nbK) * F);
+            t.nA = a.template get<int>(F); t.nbA = a.template get<int>(size_t(nbK) * F32);
             t.m1pos = a.template get<V4<R>>(Cm); t.m1slot = a.template get<int>(Cm);
             t.m1nrm = a.template get<V4<R>>(Cm); t.mcs1 = a.template get<int>(Lc);
             t.pid2 = a.template get<int>(F); t.x2 = a.template get<V4<R>>(F);
             t.u2 = a.template get<V4<R>>(F); t.vv2 = a.template get<V4<R>>(F);
             t.P2 = a.template get<R>(F); t.vp2 = a.template get<V4<R>>(F);
-            t.nB = a.template get<int>(F); t.nbB = a.template get<int>(size_t(nbK) * F);
+            t.nB = a.template get<int>(F); t.nbB = a.template get<int>(size_t(nbK) * F32);
             t.m2pos = a.template get<V4<R>>(Cm); t.m2slot = a.template get<int>(Cm);
             t.m2nrm = a.template get<V4<R>>(Cm); t.mcs2 = a.template get<int>(Lc);
             st->tape.push_back(t);

@@ -1030,10 +1030,20 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
         col_dens_walls_mirrors<R, RN, true, true>(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.wl, a.m,
                                                   a.skip != 0, wx, wy, wz, ni, cnt5);
     } else {
-        int t5[5] = {0, 0, 0, 0, 0};  // a separate array keeps cnt5 in registers
+        // The out-of-line walk takes its sums by reference, so it gets copies: a variable whose
+        // address reaches a call lives in local memory, and the sums of the list path above
+        // would then be read and written there for every neighbour (measured: about 650 bytes
+        // of local stores per particle in this pass).
+        int t5[5] = {0, 0, 0, 0, 0};
+        R tx = wx, ty = wy, tz = wz;
+        RN tn = ni;
         col_dens_sum_outline<R, RN, true, true>(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.csr,
-                                                a.posf, a.vel, a.wl, a.m, a.skip != 0, wx, wy, wz,
-                                                ni, t5);
+                                                a.posf, a.vel, a.wl, a.m, a.skip != 0, tx, ty, tz,
+                                                tn, t5);
+        wx = tx;
+        wy = ty;
+        wz = tz;
+        ni = tn;
 #pragma unroll
         for (int k = 0; k < 5; ++k) cnt5[k] = t5[k];
     }
@@ -1134,8 +1144,15 @@ __global__ void __launch_bounds__(128, CORR ? 6 : 8) k_pass_c(PassArgs<R, RN> a)
         }
         grad_sum_mirrors(sc, c, pid - sc.pbase, p.x, p.y, p.z, pmin, a.m, a.skip != 0, g, cm);
     } else {
+        // copies for the out-of-line walk, which takes them by reference: the list path's
+        // sums stay in registers (see k_pass_b)
+        G g2 = g;
+        int cf2 = cf, cm2 = cm;
         grad_sum_outline(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, pi, a.csr, a.posf, a.tprs, a.m,
-                         a.skip != 0, g, cf, cm);
+                         a.skip != 0, g2, cf2, cm2);
+        g = g2;
+        cf = cf2;
+        cm = cm2;
     }
     V4<R> v = a.tvel[s];
     R ax, ay, az;

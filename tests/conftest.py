@@ -22,8 +22,43 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (runs the sm_100a library)")
 
 
+_GOLDEN_CACHE = {}
+
+
 def golden(prec: str) -> dict:
-    return dict(np.load(os.path.join(GOLDEN, f"ref_small_{prec}.npz")))
+    """A golden record: "f32", "f64", "corr_f32", "corr_f64" (the small scene, two steps) or
+    "6k_f64" (the 6 000-particle dam break, its second step; see golden_6k)."""
+    if prec not in _GOLDEN_CACHE:
+        if prec == "6k_f64":
+            _GOLDEN_CACHE[prec] = golden_6k()
+        else:
+            _GOLDEN_CACHE[prec] = dict(np.load(os.path.join(GOLDEN, f"ref_small_{prec}.npz")))
+    return _GOLDEN_CACHE[prec]
+
+
+def golden_6k() -> dict:
+    """ref_6k_f64.npz expanded to the layout of the small records. The file stores the state
+    before the step whole and after each method only what changed; the particles themselves
+    are the workload's seeded scene, regenerated here (its checksum is in the file)."""
+    from oracle import scenes
+    path = os.path.join(GOLDEN, "ref_6k_f64.npz")
+    if not os.path.exists(path):
+        pytest.skip("ref_6k_f64.npz not recorded (tests/golden/make_golden.py --6k)")
+    z = dict(np.load(path))
+    scene, _, _ = scenes.WORKLOADS[str(z["workload"])]
+    sc = scenes.dambreak(scene)
+    nf = int(z["nf"])
+    got = np.array([float(sc["pos"].sum()), float(sc["nrm"].sum()), nf])
+    assert np.array_equal(got, z["scene_sum"]), "the regenerated scene is not the recorded one"
+    g = dict(z)
+    g.update(typ=sc["typ"], pos=sc["pos"], vel=sc["vel"], nrm=sc["nrm"])
+    keys = ("typ", "pos", "vel", "acc", "prs", "pav", "mslot", "mpos", "mprs", "cell")
+    for s in g["record_steps"]:
+        for k in range(1, len(g["phases"]) + 1):
+            for q in keys:
+                if f"s{s}_k{k}_{q}" not in g:
+                    g[f"s{s}_k{k}_{q}"] = g[f"s{s}_k{k - 1}_{q}"]
+    return g
 
 
 def golden_params(g: dict):

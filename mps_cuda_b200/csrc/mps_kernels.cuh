@@ -477,6 +477,10 @@ __device__ __forceinline__ size_t list_at(int s, int k, int K) {
     return (size_t(s >> 5) * size_t(K) + size_t(k)) * 32 + size_t(s & 31);
 }
 
+// The step kernels take this as a `const __grid_constant__` parameter. The out-of-line walks
+// receive references to its views (wl, m); an ordinary by-value kernel parameter whose address
+// is taken is copied whole into local memory by every thread (measured: a 376-byte stack frame
+// in pass C and 480 in pass B, about 11 and 30 sectors of local stores per particle).
 template <class R, class RN> struct PassArgs {
     const SceneDev<R, RN>* sc;
     int nscene, nF, dead, skip;
@@ -878,7 +882,7 @@ __device__ __forceinline__ void pass_a_unlisted(const PassArgs<R, RN>& a, int s,
 // particle walking its candidates in global memory (posf through L1).
 // TAPE (recorded rollouts): also keeps the list length and the velocity before the clamp.
 template <class R, class RN, bool DIAG, bool TAPE = false, int NB = 4>
-__global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
+__global__ void __launch_bounds__(128) k_pass_a(const __grid_constant__ PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
     const int nalive = __ldg(a.cs + a.dead);
@@ -908,7 +912,7 @@ __global__ void __launch_bounds__(128) k_pass_a(PassArgs<R, RN> a) {
 // and with SVEL the candidates' velocities too. Same walk order and arithmetic as k_pass_a,
 // so the results are identical; blocks whose neighbourhood does not fit walk global memory.
 template <class R, class RN, bool DIAG, bool SVEL>
-__global__ void __launch_bounds__(128) k_pass_a_st(PassArgs<R, RN> a, int cap) {
+__global__ void __launch_bounds__(128) k_pass_a_st(const __grid_constant__ PassArgs<R, RN> a, int cap) {
     extern __shared__ __align__(16) unsigned char stage_mem[];
     StageHdr& h = *reinterpret_cast<StageHdr*>(stage_mem);
     V4<R>* spos = reinterpret_cast<V4<R>*>(stage_mem + ((sizeof(StageHdr) + 15) / 16) * 16);
@@ -967,7 +971,7 @@ __global__ void __launch_bounds__(128) k_pass_a_st(PassArgs<R, RN> a, int cap) {
 // pass B: ChkCol (kernel.cu:1168-1287) + MkPrs (kernel.cu:1306-1411) at x*; leaves the
 // list of fluid neighbours inside max(rp, rlim) for pass C (same positions, same slots)
 template <class R, class RN, bool DIAG>
-__global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
+__global__ void __launch_bounds__(128) k_pass_b(const __grid_constant__ PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
     const int nalive = __ldg(a.cs + a.dead);
@@ -1067,7 +1071,7 @@ __global__ void __launch_bounds__(128) k_pass_b(PassArgs<R, RN> a) {
 // reference leaves in d_Acc the velocity ChkCol stored there (kernel.cu:1275, 1620), which
 // UpPcl2 then applies as the acceleration: the velocity after pass B, as here.
 template <class R, class RN, bool DIAG, bool TAPE = false, bool CORR = false>
-__global__ void __launch_bounds__(128, CORR ? 6 : 8) k_pass_c(PassArgs<R, RN> a) {
+__global__ void __launch_bounds__(128, CORR ? 6 : 8) k_pass_c(const __grid_constant__ PassArgs<R, RN> a) {
     using G = typename std::conditional<CORR, GradCorr<R>, GradPlain<R>>::type;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
@@ -1205,7 +1209,7 @@ __device__ __forceinline__ void gen_reserve_emit(const PassArgs<R, RN>& a, const
 // pass C). Near-wall particles are a thin layer, so this runs as a light kernel of its own
 // instead of stretching the neighbour passes.
 template <class R, class RN, bool DIAG, bool TAPE = false>
-__global__ void __launch_bounds__(128, 10) k_gen_cull(PassArgs<R, RN> a, const V4<R>* gpos,
+__global__ void __launch_bounds__(128, 10) k_gen_cull(const __grid_constant__ PassArgs<R, RN> a, const V4<R>* gpos,
                                                   const R* gprs, const int8_t* gtyp) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     MirrorPlan<R> pl;
@@ -1238,7 +1242,7 @@ __global__ void __launch_bounds__(128, 10) k_gen_cull(PassArgs<R, RN> a, const V
 // reference's device arrays
 // ---------------------------------------------------------------------------------------
 template <class R, class RN, bool DIAG>
-__global__ void __launch_bounds__(128) k_ph_vsc(PassArgs<R, RN> a) {
+__global__ void __launch_bounds__(128) k_ph_vsc(const __grid_constant__ PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF || a.typ[s] != kFLD) return;
     const int pid = a.pid[s];
@@ -1261,7 +1265,7 @@ __global__ void __launch_bounds__(128) k_ph_vsc(PassArgs<R, RN> a) {
 }
 
 template <class R, class RN>
-__global__ void k_ph_uppcl1(PassArgs<R, RN> a) {
+__global__ void k_ph_uppcl1(const __grid_constant__ PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF || a.typ[s] != kFLD) return;
     const SceneDev<R, RN>& sc = scene_ref(a, a.pid[s]);
@@ -1282,7 +1286,7 @@ __global__ void k_ph_uppcl1(PassArgs<R, RN> a) {
 }
 
 template <class R, class RN, bool DIAG>
-__global__ void __launch_bounds__(128) k_ph_col(PassArgs<R, RN> a) {
+__global__ void __launch_bounds__(128) k_ph_col(const __grid_constant__ PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF || a.typ[s] != kFLD) return;
     const int pid = a.pid[s];
@@ -1307,7 +1311,7 @@ __global__ void __launch_bounds__(128) k_ph_col(PassArgs<R, RN> a) {
 
 // d_UpChkCol (kernel.cu:1281-1287): Acc holds the corrected velocity, Vel = Acc
 template <class R, class RN>
-__global__ void k_ph_upchkcol(PassArgs<R, RN> a) {
+__global__ void k_ph_upchkcol(const __grid_constant__ PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF || a.typ[s] != kFLD) return;
     V4<R> w = a.tvel[s];
@@ -1316,7 +1320,7 @@ __global__ void k_ph_upchkcol(PassArgs<R, RN> a) {
 }
 
 template <class R, class RN, bool DIAG>
-__global__ void __launch_bounds__(128) k_ph_prs(PassArgs<R, RN> a) {
+__global__ void __launch_bounds__(128) k_ph_prs(const __grid_constant__ PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF || a.typ[s] != kFLD) return;
     const int pid = a.pid[s];
@@ -1340,7 +1344,7 @@ __global__ void __launch_bounds__(128) k_ph_prs(PassArgs<R, RN> a) {
 }
 
 template <class R, class RN, bool DIAG, bool CORR = false>
-__global__ void __launch_bounds__(128) k_ph_grd(PassArgs<R, RN> a) {
+__global__ void __launch_bounds__(128) k_ph_grd(const __grid_constant__ PassArgs<R, RN> a) {
     using G = typename std::conditional<CORR, GradCorr<R>, GradPlain<R>>::type;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF || a.typ[s] != kFLD) return;
@@ -1364,7 +1368,7 @@ __global__ void __launch_bounds__(128) k_ph_grd(PassArgs<R, RN> a) {
 }
 
 template <class R, class RN>
-__global__ void k_ph_uppcl2(PassArgs<R, RN> a) {
+__global__ void k_ph_uppcl2(const __grid_constant__ PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
     if (a.typ[s] == kFLD) {
@@ -1392,7 +1396,7 @@ __global__ void k_ph_uppcl2(PassArgs<R, RN> a) {
 
 // GenMRR_nonslip without the cull (the cull is MkBkt_MRR's d_MRRinout)
 template <class R, class RN, bool DIAG>
-__global__ void __launch_bounds__(128) k_ph_gen(PassArgs<R, RN> a) {
+__global__ void __launch_bounds__(128) k_ph_gen(const __grid_constant__ PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     MirrorPlan<R> pl;
     pl.nreg = 0;
@@ -1454,7 +1458,7 @@ __device__ __forceinline__ void nearest_wall_part(const SceneDev<R, RN>& sc, con
 // keeps the smallest distance, on ties the earlier row, which is the wall the sequential
 // walk keeps (the first nearest one found).
 template <class R, class RN>
-__global__ void k_ph_cull(PassArgs<R, RN> a) {
+__global__ void k_ph_cull(const __grid_constant__ PassArgs<R, RN> a) {
     const int n = min(a.cnt->mirror_raw, a.out.cap);
     const int part = threadIdx.x & 3;
     const int groups = (gridDim.x * blockDim.x) >> 2;

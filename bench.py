@@ -368,6 +368,11 @@ def run_ours(args, world, rank, local):
     # the library's tuned shapes for this scene (mps_autotune restores the state it tried
     # them on), as a user calls it once per handle
     tuned = None if args.no_tune else g.autotune(3)
+    # shapes forced from the command line (profiling one variant), after the tuner
+    if args.staging is not None:
+        g.set_option(L.OPT_STAGING, args.staging)
+    if args.candidate_batch is not None:
+        g.set_option(L.OPT_CANDIDATE_BATCH, args.candidate_batch)
     g.set_option(L.OPT_GRAPH, 1)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
@@ -540,6 +545,7 @@ def measure_workload(workload: str, precision: str, stream, flush, K: int):
     nf = int((typ == 0).sum())
     g = MPS(p, typ, pos, vel, nrm)
     g.set_stream(stream.cuda_stream)
+    tuned = g.autotune(3)  # as for the headline workload: the handle's own tuned shapes
     g.set_option(L.OPT_GRAPH, 1)
     for _ in range(3):
         g.step(1)
@@ -567,7 +573,7 @@ def measure_workload(workload: str, precision: str, stream, flush, K: int):
             "wall_particles": int((typ != 0).sum()), "steps": K, "ms_per_step": ms,
             "value": nf / (ms / 1e3), "unit": "particle-updates/s",
             "kernel_groups_ms_per_launch": {k: v[0] / v[1] for k, v in tm.items() if v[1]},
-            "deleted": cnt["n_deleted"], "errors": {k: v for k, v in cnt.items() if k.startswith("err")}}
+            "tuned_shapes": tuned, "deleted": cnt["n_deleted"], "errors": {k: v for k, v in cnt.items() if k.startswith("err")}}
 
 
 def measure_adjoint(stream):
@@ -747,6 +753,10 @@ def main():
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--no-compute", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--staging", type=int, choices=[0, 1, 2], default=None,
+                    help="force pass A's staging mode (0 global, 1 positions, 2 velocities)")
+    ap.add_argument("--candidate-batch", type=int, choices=[2, 4, 8], default=None,
+                    help="force pass A's candidates per batch")
     args = ap.parse_args()
     world, rank, local = setup_dist()
     try:

@@ -163,8 +163,12 @@ enum {
     MPS_OPT_STAGE_CAPACITY = 8, /* candidates a block may stage in shared memory (0 = the
                                 default); a block whose neighbourhood holds more walks
                                 global memory. Results never depend on it.               */
-    MPS_OPT_CANDIDATE_BATCH = 9 /* VscTrm's candidates loaded together per particle: 2, 4
+    MPS_OPT_CANDIDATE_BATCH = 9, /* VscTrm's candidates loaded together per particle: 2, 4
                                 or 8 (0 = 4). Results never depend on it.                */
+    MPS_OPT_REGISTER_BOUND = 10 /* bit 0: ChkCol/MkPrs, bit 1: PrsGrdTrm at their alternate
+                                register bound per thread (more or fewer resident blocks
+                                per SM; 0 = both at the default). Results never depend
+                                on it.                                                    */
 };
 
 /* MPS_OPT_STAGING. GLOBAL: each particle walks its fine cells through L1. POSITIONS: a block
@@ -322,10 +326,11 @@ int mps_get_timing(mps_handle* h, int32_t kernel, double* total_ms, int64_t* lau
  * timed over `trial_steps` steps with CUDA events and the fastest kept, per kernel group:
  * VscTrm's candidates in flight (MPS_OPT_CANDIDATE_BATCH: 2, 4, 8), threads per block (128,
  * 64) and candidate source (MPS_OPT_STAGING); ChkCol/MkPrs, PrsGrdTrm and the mirror
- * generation with 128, 96, 64 or 32 threads per block. The state is restored afterwards, so
- * tuning changes no result (no kernel's arithmetic depends on these shapes).
+ * generation with 128, 96, 64 or 32 threads per block; then ChkCol/MkPrs and PrsGrdTrm at
+ * their alternate register bound (MPS_OPT_REGISTER_BOUND). The state is restored afterwards,
+ * so tuning changes no result (no kernel's arithmetic depends on these shapes).
  * chosen[MPS_K_COUNT] receives the block sizes (may be NULL); mps_get_option reads the
- * staging mode. The choice is kept for the process: a handle created later with the same
+ * other knobs. The choice is kept for the process: a handle created later with the same
  * precision, batched or not, and fluid count in the same power-of-two class starts from it.
  */
 int mps_autotune(mps_handle* h, int32_t trial_steps, int32_t* chosen);

@@ -202,6 +202,12 @@ int mps_set_option(mps_handle* h, int32_t opt, int32_t value) {
                 s.batch_a = value ? value : 4;
                 s.invalidate_graph();
                 break;
+            case MPS_OPT_REGISTER_BOUND:
+                if (value < 0 || value > 3)
+                    throw ApiError(MPS_ERR_ARG, "register bound must lie in [0, 3]");
+                s.reg_bound = value;
+                s.invalidate_graph();
+                break;
             case MPS_OPT_STAGE_CAPACITY:
                 if (value < 0 || value > (1 << 16))
                     throw ApiError(MPS_ERR_ARG, "stage capacity must lie in [0, 65536]");
@@ -233,6 +239,7 @@ int mps_get_option(mps_handle* h, int32_t opt, int32_t* value) {
             case MPS_OPT_STAGING: *value = s.stage_mode; break;
             case MPS_OPT_STAGE_CAPACITY: *value = s.stage_cap; break;
             case MPS_OPT_CANDIDATE_BATCH: *value = s.batch_a; break;
+            case MPS_OPT_REGISTER_BOUND: *value = s.reg_bound; break;
             default: throw ApiError(MPS_ERR_ARG, "unknown option");
         }
     });

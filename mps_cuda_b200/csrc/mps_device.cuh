@@ -415,21 +415,6 @@ __device__ __forceinline__ void col_dens_sum(const SceneDev<R, RN>& sc, const Ro
                                              ni, cnt);
 }
 
-// out-of-line copy for the rare slot whose neighbour list overflowed its capacity: keeps
-// the scan's code out of the list-walking kernel's instruction stream
-template <class R, class RN, bool COL, bool DENS>
-__device__ __noinline__ void col_dens_sum_outline(const SceneDev<R, RN>& sc, const RowCtx<R>& c,
-                                                  int s, R x, R y, R z, R ux, R uy, R uz,
-                                                  const int* __restrict__ csr,
-                                                  const V4<R>* __restrict__ posf,
-                                                  const V4<R>* __restrict__ vel,
-                                                  const WallView<R>& wl, const MirrorView<R>& m,
-                                                  bool skip, R& wx, R& wy, R& wz, RN& ni,
-                                                  int* cnt) {
-    col_dens_sum<R, RN, COL, DENS>(sc, c, s, x, y, z, ux, uy, uz, csr, posf, vel, wl, m, skip, wx,
-                                   wy, wz, ni, cnt);
-}
-
 // explicit equation of state with clamps, kernel.cu:1388-1406
 template <class R, class RN>
 __device__ __forceinline__ R eos(const SceneDev<R, RN>& sc, RN ni) {
@@ -559,17 +544,6 @@ __device__ __forceinline__ void grad_sum(const SceneDev<R, RN>& sc, const RowCtx
         }
     });
     grad_sum_mirrors(sc, c, pid_local, x, y, z, pmin, m, skip, g, cm);
-}
-
-// out-of-line copy for the rare slot whose neighbour list overflowed its capacity
-template <class R, class RN, class G>
-__device__ __noinline__ void grad_sum_outline(const SceneDev<R, RN>& sc, const RowCtx<R>& c, int s,
-                                              int pid_local, R x, R y, R z, R pi,
-                                              const int* __restrict__ csr,
-                                              const V4<R>* __restrict__ posf,
-                                              const R* __restrict__ prs, const MirrorView<R>& m,
-                                              bool skip, G& g, int& cf, int& cm) {
-    grad_sum(sc, c, s, pid_local, x, y, z, pi, csr, posf, prs, m, skip, g, cf, cm);
 }
 
 // ---- GenMRR_nonslip for one fluid particle (kernel.cu:726-891) ---------------------------

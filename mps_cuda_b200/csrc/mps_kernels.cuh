@@ -477,6 +477,25 @@ __device__ __forceinline__ size_t list_at(int s, int k, int K) {
     return (size_t(s >> 5) * size_t(K) + size_t(k)) * 32 + size_t(s & 31);
 }
 
+// Resident blocks per SM asked of a kernel tuned in FP32: half as many in FP64, whose values
+// take two registers each (at the FP32 bound the FP64 kernels spill).
+template <class R> constexpr int min_blocks(int f32) { return sizeof(R) == 8 ? f32 / 2 : f32; }
+
+// Two register bounds each for passes B and C (MPS_OPT_REGISTER_BOUND, chosen by the
+// autotuner); which is faster depends on the grid's size and the precision. Pass B: the
+// registers the compiler wants (FP32 64, FP64 96), or about one more resident block per SM
+// with a few spills (FP32 56, FP64 80). Pass C: 8 blocks per SM (FP32 64 registers without
+// spills, FP64 64 with about 200 bytes of spills), or FP32 10 blocks (48) and FP64 4 blocks
+// (122, no spills). Measured with CUDA events: at 6.1M particles in FP32 the alternate bounds
+// take pass B from 2.34 to 2.09 ms and pass C from 1.18 to 1.11 ms; in FP64 the spill-free
+// pass C is 9 % faster at 48 000 particles and 10 % slower at 384 000.
+template <class R> constexpr int pass_b_blocks(bool alt) {
+    return alt ? (sizeof(R) == 8 ? 6 : 9) : 1;
+}
+template <class R> constexpr int pass_c_blocks(bool alt, bool corr) {
+    return corr ? min_blocks<R>(6) : alt ? (sizeof(R) == 8 ? 4 : 10) : 8;
+}
+
 // The step kernels take this as a `const __grid_constant__` parameter. The out-of-line walks
 // receive references to its views (wl, m); an ordinary by-value kernel parameter whose address
 // is taken is copied whole into local memory by every thread (measured: a 376-byte stack frame
@@ -968,10 +987,49 @@ __global__ void __launch_bounds__(128) k_pass_a_st(const __grid_constant__ PassA
     pass_a_finish<R, RN, DIAG, false>(a, sc, s, pid, p, v, c, sx, sy, sz, cf);
 }
 
+// pass B's stores: velocity after ChkCol, pressure from MkPrs's EOS, diagnostics
+template <class R, class RN, bool DIAG>
+__device__ __forceinline__ void pass_b_store(const PassArgs<R, RN>& a, const SceneDev<R, RN>& sc,
+                                             int s, int pid, R wx, R wy, R wz, RN ni,
+                                             const int* cnt5) {
+    a.tvel[s] = V4<R>{wx, wy, wz, R(0)};
+    a.tprs[s] = eos(sc, ni);
+    if (DIAG) {
+        int32_t* d = a.diag + size_t(pid) * kDiagCols;
+        d[DG_COL_F] = cnt5[0];
+        d[DG_COL_W] = cnt5[1];
+        d[DG_COL_M] = cnt5[2];
+        d[DG_PRS_F] = cnt5[3];
+        d[DG_PRS_M] = cnt5[4];
+        a.ndens[pid] = ni;
+    }
+}
+
+// Pass B for the rare slot whose list overflowed its capacity: scans the fine rows again and
+// finishes the slot. Out of line, and the last thing its caller does: nothing of the caller's
+// stays live across the call, so the list path keeps its values in registers (a call that
+// returns sums by reference, or has values live across it, puts them in local memory).
+template <class R, class RN, bool DIAG>
+__device__ __noinline__ void pass_b_long(const PassArgs<R, RN>& a, int s) {
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    const V4<R> p = ldg4(a.pos + s), v = ldg4(a.vel + s);
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    const RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    R wx = v.x, wy = v.y, wz = v.z;
+    RN ni = 0;
+    int cnt5[5] = {0, 0, 0, 0, 0};
+    col_dens_sum<R, RN, true, true>(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.csr, a.posf, a.vel,
+                                    a.wl, a.m, a.skip != 0, wx, wy, wz, ni, cnt5);
+    pass_b_store<R, RN, DIAG>(a, sc, s, pid, wx, wy, wz, ni, cnt5);
+}
+
 // pass B: ChkCol (kernel.cu:1168-1287) + MkPrs (kernel.cu:1306-1411) at x*; leaves the
 // list of fluid neighbours inside max(rp, rlim) for pass C (same positions, same slots)
-template <class R, class RN, bool DIAG>
-__global__ void __launch_bounds__(128) k_pass_b(const __grid_constant__ PassArgs<R, RN> a) {
+template <class R, class RN, bool DIAG, bool ALT = false>
+__global__ void __launch_bounds__(128, pass_b_blocks<R>(ALT))
+    k_pass_b(const __grid_constant__ PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
     const int nalive = __ldg(a.cs + a.dead);
@@ -986,9 +1044,6 @@ __global__ void __launch_bounds__(128) k_pass_b(const __grid_constant__ PassArgs
     int ix, iy, iz;
     cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
     RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
-    R wx = v.x, wy = v.y, wz = v.z;
-    RN ni = 0;
-    int cnt5[5] = {0, 0, 0, 0, 0};
     int ncand = 0;
     const int n = build_list<R, RN, DIAG>(a, sc, c, s, p.x, p.y, p.z, sc.list_thr,
                                           MPS_INF_SKIP(a, sc.skip_rc), &ncand);
@@ -997,167 +1052,57 @@ __global__ void __launch_bounds__(128) k_pass_b(const __grid_constant__ PassArgs
         warp_add_u64(&a.cnt->work[1], ncand);
         warp_add_u64(&a.cnt->work[2], n);
     }
-    if (n <= a.nbK) {
-        const int* __restrict__ nb = a.nb + list_at(s, 0, a.nbK);
-        const V4<R>* __restrict__ pos = a.pos;
-        const V4<R>* __restrict__ vel = a.vel;
-        const int st = 32;
-        const R rlim2 = sc.rlim2, rp_lt = sc.rp_lt, colfac = sc.colfac, rp = sc.rp;
-        const RN rp_n = sc.rp_n;
-        auto add = [&](int j, const V4<R>& q) {
-            R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-            R d2 = dot3(dx, dy, dz, dx, dy, dz);
-            if (d2 < rlim2) {
-                V4<R> u = ldg4(vel + j);
-                col_hit(colfac, v.x, v.y, v.z, u.x, u.y, u.z, dx, dy, dz, d2, wx, wy, wz);
-                ++cnt5[0];
-            }
-            if (d2 <= rp_lt) {
-                dens_add_v(rp, rp_n, d2, ni);
-                ++cnt5[3];
-            }
-        };
-        int k = 0;
-        for (; k + 4 <= n; k += 4) {
-            const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
-                      j3 = nb[(k + 3) * st];
-            V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
-            add(j0, q0);
-            add(j1, q1);
-            add(j2, q2);
-            add(j3, q3);
-        }
-        for (; k < n; ++k) {
-            const int j = nb[k * st];
-            add(j, ldg4(pos + j));
-        }
-        col_dens_walls_mirrors<R, RN, true, true>(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.wl, a.m,
-                                                  a.skip != 0, wx, wy, wz, ni, cnt5);
-    } else {
-        // The out-of-line walk takes its sums by reference, so it gets copies: a variable whose
-        // address reaches a call lives in local memory, and the sums of the list path above
-        // would then be read and written there for every neighbour (measured: about 650 bytes
-        // of local stores per particle in this pass).
-        int t5[5] = {0, 0, 0, 0, 0};
-        R tx = wx, ty = wy, tz = wz;
-        RN tn = ni;
-        col_dens_sum_outline<R, RN, true, true>(sc, c, s, p.x, p.y, p.z, v.x, v.y, v.z, a.csr,
-                                                a.posf, a.vel, a.wl, a.m, a.skip != 0, tx, ty, tz,
-                                                tn, t5);
-        wx = tx;
-        wy = ty;
-        wz = tz;
-        ni = tn;
-#pragma unroll
-        for (int k = 0; k < 5; ++k) cnt5[k] = t5[k];
-    }
-    R P = eos(sc, ni);
-    a.tvel[s] = V4<R>{wx, wy, wz, R(0)};
-    a.tprs[s] = P;
-    if (DIAG) {
-        int32_t* d = a.diag + size_t(pid) * kDiagCols;
-        d[DG_COL_F] = cnt5[0];
-        d[DG_COL_W] = cnt5[1];
-        d[DG_COL_M] = cnt5[2];
-        d[DG_PRS_F] = cnt5[3];
-        d[DG_PRS_M] = cnt5[4];
-        a.ndens[pid] = ni;
-    }
-}
-
-// pass C: PrsGrdTrm (kernel.cu:1651-1794) + UpPcl2/ChkPcl (kernel.cu:1815-1829), walking
-// the neighbour lists pass B left. TAPE: also keeps the velocity before the clamp. CORR: the
-// corrected-matrix PrsGrdTrm (kernel.cu:1435-1648); where its moment matrix is all zero the
-// reference leaves in d_Acc the velocity ChkCol stored there (kernel.cu:1275, 1620), which
-// UpPcl2 then applies as the acceleration: the velocity after pass B, as here.
-template <class R, class RN, bool DIAG, bool TAPE = false, bool CORR = false>
-__global__ void __launch_bounds__(128, CORR ? 6 : 8) k_pass_c(const __grid_constant__ PassArgs<R, RN> a) {
-    using G = typename std::conditional<CORR, GradCorr<R>, GradPlain<R>>::type;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.nF) return;
-    const int nalive = __ldg(a.cs + a.dead);
-    if (s >= nalive) {
-        a.tpos[s] = a.pos[s];
-        a.ttyp[s] = a.typ[s];
-        if (TAPE) a.tape_pre[s] = V4<R>{R(0), R(0), R(0), R(kTapeDead)};
+    if (n > a.nbK) {
+        pass_b_long<R, RN, DIAG>(a, s);
         return;
     }
-    const int pid = a.pid[s];
-    const SceneDev<R, RN>& sc = scene_ref(a, pid);
-    V4<R> p = ldg4(a.pos + s);
-    const R pi = a.tprs[s];
-    int ix, iy, iz;
-    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
-    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
-    G g;
-    int cf = 0, cm = 0;
-    const int n = a.nbcnt[s];
-    if (n <= a.nbK) {
-        const int* __restrict__ nb = a.nb + list_at(s, 0, a.nbK);
-        const V4<R>* __restrict__ pos = a.pos;
-        const R* __restrict__ prs = a.tprs;
-        const int st = 32;
-        const R rp2 = sc.rp2, rp = sc.rp;
-        // P_min over the fluid neighbours inside rp (order-free), then the gradient in order
-        R pmin = pi;
-        // each list entry's position and pressure are loaded together (both depend only on
-        // the index), four entries in flight, before the tests that use them
-        auto mn = [&](const V4<R>& q, R pj) {
-            R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-            if (dot3(dx, dy, dz, dx, dy, dz) < rp2 && pj < pmin) pmin = pj;
-        };
-        int k = 0;
-        for (; k + 4 <= n; k += 4) {
-            const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
-                      j3 = nb[(k + 3) * st];
-            V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
-            const R r0 = __ldg(prs + j0), r1 = __ldg(prs + j1), r2 = __ldg(prs + j2),
-                    r3 = __ldg(prs + j3);
-            mn(q0, r0);
-            mn(q1, r1);
-            mn(q2, r2);
-            mn(q3, r3);
+    R wx = v.x, wy = v.y, wz = v.z;
+    RN ni = 0;
+    int cnt5[5] = {0, 0, 0, 0, 0};
+    const int* __restrict__ nb = a.nb + list_at(s, 0, a.nbK);
+    const V4<R>* __restrict__ pos = a.pos;
+    const V4<R>* __restrict__ vel = a.vel;
+    const int st = 32;
+    const R rlim2 = sc.rlim2, rp_lt = sc.rp_lt, colfac = sc.colfac, rp = sc.rp;
+    const RN rp_n = sc.rp_n;
+    auto add = [&](int j, const V4<R>& q) {
+        R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (d2 < rlim2) {
+            V4<R> u = ldg4(vel + j);
+            col_hit(colfac, v.x, v.y, v.z, u.x, u.y, u.z, dx, dy, dz, d2, wx, wy, wz);
+            ++cnt5[0];
         }
-        for (; k < n; ++k) {
-            const int j = nb[k * st];
-            mn(ldg4(pos + j), __ldg(prs + j));
+        if (d2 <= rp_lt) {
+            dens_add_v(rp, rp_n, d2, ni);
+            ++cnt5[3];
         }
-        auto gr = [&](const V4<R>& q, R pj) {
-            R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-            R d2 = dot3(dx, dy, dz, dx, dy, dz);
-            if (d2 < rp2) {
-                R d = sqrtR(d2);
-                g.add(wei_grad(d, rp) / d2, pj - pmin, dx, dy, dz);
-                ++cf;
-            }
-        };
-        for (k = 0; k + 4 <= n; k += 4) {
-            const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
-                      j3 = nb[(k + 3) * st];
-            V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
-            const R r0 = __ldg(prs + j0), r1 = __ldg(prs + j1), r2 = __ldg(prs + j2),
-                    r3 = __ldg(prs + j3);
-            gr(q0, r0);
-            gr(q1, r1);
-            gr(q2, r2);
-            gr(q3, r3);
-        }
-        for (; k < n; ++k) {
-            const int j = nb[k * st];
-            gr(ldg4(pos + j), __ldg(prs + j));
-        }
-        grad_sum_mirrors(sc, c, pid - sc.pbase, p.x, p.y, p.z, pmin, a.m, a.skip != 0, g, cm);
-    } else {
-        // copies for the out-of-line walk, which takes them by reference: the list path's
-        // sums stay in registers (see k_pass_b)
-        G g2 = g;
-        int cf2 = cf, cm2 = cm;
-        grad_sum_outline(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, pi, a.csr, a.posf, a.tprs, a.m,
-                         a.skip != 0, g2, cf2, cm2);
-        g = g2;
-        cf = cf2;
-        cm = cm2;
+    };
+    int k = 0;
+    for (; k + 4 <= n; k += 4) {
+        const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
+                  j3 = nb[(k + 3) * st];
+        V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
+        add(j0, q0);
+        add(j1, q1);
+        add(j2, q2);
+        add(j3, q3);
     }
+    for (; k < n; ++k) {
+        const int j = nb[k * st];
+        add(j, ldg4(pos + j));
+    }
+    col_dens_walls_mirrors<R, RN, true, true>(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.wl, a.m,
+                                              a.skip != 0, wx, wy, wz, ni, cnt5);
+    pass_b_store<R, RN, DIAG>(a, sc, s, pid, wx, wy, wz, ni, cnt5);
+}
+
+// pass C's end for one slot: acceleration from the gradient sums, UpPcl2 (kick and drift),
+// ChkPcl, stores and diagnostics
+template <class R, class RN, bool DIAG, bool TAPE, class G>
+__device__ __forceinline__ void pass_c_finish(const PassArgs<R, RN>& a, const SceneDev<R, RN>& sc,
+                                              int s, int pid, const V4<R>& p, R pi, const G& g,
+                                              int cf, int cm) {
     V4<R> v = a.tvel[s];
     R ax, ay, az;
     if (!grad_acc(sc, g, ax, ay, az)) {
@@ -1185,6 +1130,113 @@ __global__ void __launch_bounds__(128, CORR ? 6 : 8) k_pass_c(const __grid_const
     }
 }
 
+// Pass C for a slot whose list overflowed its capacity: the fine-row scan, then the slot's
+// end; out of line and a tail call, like pass_b_long
+template <class R, class RN, bool DIAG, bool TAPE, class G>
+__device__ __noinline__ void pass_c_long(const PassArgs<R, RN>& a, int s) {
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    const V4<R> p = ldg4(a.pos + s);
+    const R pi = a.tprs[s];
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    const RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    G g;
+    int cf = 0, cm = 0;
+    grad_sum(sc, c, s, pid - sc.pbase, p.x, p.y, p.z, pi, a.csr, a.posf, a.tprs, a.m,
+             a.skip != 0, g, cf, cm);
+    pass_c_finish<R, RN, DIAG, TAPE>(a, sc, s, pid, p, pi, g, cf, cm);
+}
+
+// pass C: PrsGrdTrm (kernel.cu:1651-1794) + UpPcl2/ChkPcl (kernel.cu:1815-1829), walking
+// the neighbour lists pass B left. TAPE: also keeps the velocity before the clamp. CORR: the
+// corrected-matrix PrsGrdTrm (kernel.cu:1435-1648); where its moment matrix is all zero the
+// reference leaves in d_Acc the velocity ChkCol stored there (kernel.cu:1275, 1620), which
+// UpPcl2 then applies as the acceleration: the velocity after pass B, as here.
+template <class R, class RN, bool DIAG, bool TAPE = false, bool CORR = false, bool ALT = false>
+__global__ void __launch_bounds__(128, pass_c_blocks<R>(ALT, CORR))
+    k_pass_c(const __grid_constant__ PassArgs<R, RN> a) {
+    using G = typename std::conditional<CORR, GradCorr<R>, GradPlain<R>>::type;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nF) return;
+    const int nalive = __ldg(a.cs + a.dead);
+    if (s >= nalive) {
+        a.tpos[s] = a.pos[s];
+        a.ttyp[s] = a.typ[s];
+        if (TAPE) a.tape_pre[s] = V4<R>{R(0), R(0), R(0), R(kTapeDead)};
+        return;
+    }
+    const int n = a.nbcnt[s];
+    if (n > a.nbK) {
+        pass_c_long<R, RN, DIAG, TAPE, G>(a, s);
+        return;
+    }
+    const int pid = a.pid[s];
+    const SceneDev<R, RN>& sc = scene_ref(a, pid);
+    V4<R> p = ldg4(a.pos + s);
+    const R pi = a.tprs[s];
+    int ix, iy, iz;
+    cell_of(sc, p.x, p.y, p.z, ix, iy, iz);
+    RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
+    G g;
+    int cf = 0, cm = 0;
+    const int* __restrict__ nb = a.nb + list_at(s, 0, a.nbK);
+    const V4<R>* __restrict__ pos = a.pos;
+    const R* __restrict__ prs = a.tprs;
+    const int st = 32;
+    const R rp2 = sc.rp2, rp = sc.rp;
+    // P_min over the fluid neighbours inside rp (order-free), then the gradient in order
+    R pmin = pi;
+    // each list entry's position and pressure are loaded together (both depend only on
+    // the index), four entries in flight, before the tests that use them
+    auto mn = [&](const V4<R>& q, R pj) {
+        R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+        if (dot3(dx, dy, dz, dx, dy, dz) < rp2 && pj < pmin) pmin = pj;
+    };
+    int k = 0;
+    for (; k + 4 <= n; k += 4) {
+        const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
+                  j3 = nb[(k + 3) * st];
+        V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
+        const R r0 = __ldg(prs + j0), r1 = __ldg(prs + j1), r2 = __ldg(prs + j2),
+                r3 = __ldg(prs + j3);
+        mn(q0, r0);
+        mn(q1, r1);
+        mn(q2, r2);
+        mn(q3, r3);
+    }
+    for (; k < n; ++k) {
+        const int j = nb[k * st];
+        mn(ldg4(pos + j), __ldg(prs + j));
+    }
+    auto gr = [&](const V4<R>& q, R pj) {
+        R dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+        R d2 = dot3(dx, dy, dz, dx, dy, dz);
+        if (d2 < rp2) {
+            R d = sqrtR(d2);
+            g.add(wei_grad(d, rp) / d2, pj - pmin, dx, dy, dz);
+            ++cf;
+        }
+    };
+    for (k = 0; k + 4 <= n; k += 4) {
+        const int j0 = nb[k * st], j1 = nb[(k + 1) * st], j2 = nb[(k + 2) * st],
+                  j3 = nb[(k + 3) * st];
+        V4<R> q0 = ldg4(pos + j0), q1 = ldg4(pos + j1), q2 = ldg4(pos + j2), q3 = ldg4(pos + j3);
+        const R r0 = __ldg(prs + j0), r1 = __ldg(prs + j1), r2 = __ldg(prs + j2),
+                r3 = __ldg(prs + j3);
+        gr(q0, r0);
+        gr(q1, r1);
+        gr(q2, r2);
+        gr(q3, r3);
+    }
+    for (; k < n; ++k) {
+        const int j = nb[k * st];
+        gr(ldg4(pos + j), __ldg(prs + j));
+    }
+    grad_sum_mirrors(sc, c, pid - sc.pbase, p.x, p.y, p.z, pmin, a.m, a.skip != 0, g, cm);
+    pass_c_finish<R, RN, DIAG, TAPE>(a, sc, s, pid, p, pi, g, cf, cm);
+}
+
 // The warp's mirrors take consecutive places in the raw list, reserved with one atomic per
 // warp (the list's order does not matter: the mirror bucket build sorts by bucket and slot).
 // Every lane of the warp calls this.
@@ -1209,7 +1261,7 @@ __device__ __forceinline__ void gen_reserve_emit(const PassArgs<R, RN>& a, const
 // pass C). Near-wall particles are a thin layer, so this runs as a light kernel of its own
 // instead of stretching the neighbour passes.
 template <class R, class RN, bool DIAG, bool TAPE = false>
-__global__ void __launch_bounds__(128, 10) k_gen_cull(const __grid_constant__ PassArgs<R, RN> a, const V4<R>* gpos,
+__global__ void __launch_bounds__(128, min_blocks<R>(10)) k_gen_cull(const __grid_constant__ PassArgs<R, RN> a, const V4<R>* gpos,
                                                   const R* gprs, const int8_t* gtyp) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     MirrorPlan<R> pl;

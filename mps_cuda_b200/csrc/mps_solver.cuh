@@ -273,6 +273,7 @@ struct SolverBase {
     int stage_mode = MPS_STAGE_GLOBAL;  // pass A's candidate source (MPS_OPT_STAGING)
     int stage_cap = 0;                  // candidates staged per block (MPS_OPT_STAGE_CAPACITY)
     int batch_a = 4;                    // VscTrm's candidates in flight (MPS_OPT_CANDIDATE_BATCH)
+    int reg_bound = 0;                  // passes B, C at their alternate register bound (bits 0, 1)
     long long steps = 0;
     long long launches = 0;       // kernels launched (graph replays included)
     long long body_launches = 0;  // kernels of one captured step
@@ -329,7 +330,7 @@ struct TuneKey {
 };
 struct Tuned {
     int blk[MPS_K_COUNT];
-    int stage, batch;
+    int stage, batch, regb;
 };
 bool tuned_cache_get(const TuneKey& k, Tuned* out);
 void tuned_cache_put(const TuneKey& k, const Tuned& t);
@@ -562,6 +563,7 @@ template <class R, class RN> class Solver final : public SolverBase {
             for (int k = 0; k < MPS_K_COUNT; ++k) blk[k] = t.blk[k];
             stage_mode = t.stage;
             batch_a = t.batch;
+            reg_bound = t.regb;
         }
     }
 
@@ -836,7 +838,10 @@ template <class R, class RN> class Solver final : public SolverBase {
         // pass B: ChkCol + MkPrs, then the second mirror generation at (x*, P)
         {
             Scope t(this, MPS_K_PASS_B);
-            k_pass_b<R, RN, D><<<blocks(nF, bb), bb, 0, stream>>>(args(M1, mcs1));
+            if (reg_bound & 1)
+                k_pass_b<R, RN, D, true><<<blocks(nF, bb), bb, 0, stream>>>(args(M1, mcs1));
+            else
+                k_pass_b<R, RN, D><<<blocks(nF, bb), bb, 0, stream>>>(args(M1, mcs1));
             KL();
         }
         reset_raw();
@@ -854,6 +859,9 @@ template <class R, class RN> class Solver final : public SolverBase {
             Scope t(this, MPS_K_PASS_C);
             if (grad_mode == MPS_GRAD_CORRECTED)
                 k_pass_c<R, RN, D, false, true><<<blocks(nF, bc), bc, 0, stream>>>(args(M2, mcs2));
+            else if (reg_bound & 2)
+                k_pass_c<R, RN, D, false, false, true><<<blocks(nF, bc), bc, 0, stream>>>(
+                    args(M2, mcs2));
             else
                 k_pass_c<R, RN, D><<<blocks(nF, bc), bc, 0, stream>>>(args(M2, mcs2));
             KL();
@@ -897,7 +905,8 @@ template <class R, class RN> class Solver final : public SolverBase {
     // Autotuner. Candidates per kernel group, each timed over `trial` steps with CUDA events:
     //   pass A (VscTrm): candidates in flight (2, 4, 8) and 128 or 64 threads per block
     //                    for the walk through L1, and the staged walk at 128 threads;
-    //   passes B, C and mirror generation: 128, 96, 64 or 32 threads per block.
+    //   passes B, C and mirror generation: 128, 96, 64 or 32 threads per block;
+    //   then passes B and C at their alternate register bound, with the chosen block sizes.
     // All groups are timed in the same trial steps (they are separate kernels). The state is
     // restored afterwards, and the choice is kept for later handles of the same precision
     // and size class in this process (tuned_cache).
@@ -912,6 +921,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         int bestb[MPS_K_COUNT];
         for (int k = 0; k < MPS_K_COUNT; ++k) { best[k] = 1e300; bestb[k] = blk[k]; }
         int best_stage = stage_mode, best_batch = batch_a;
+        reg_bound = 0;
         store_all();  // snapshot of the state in the id-order staging buffers
         const long long steps0 = steps;
         const bool timing0 = timing_on;
@@ -952,13 +962,29 @@ template <class R, class RN> class Solver final : public SolverBase {
         blk[MPS_K_PASS_A] = bestb[MPS_K_PASS_A];
         stage_mode = best_stage;
         batch_a = best_batch;
+        // the alternate register bounds of passes B and C, at the chosen shapes
+        reg_bound = 3;
+        step(trial);
+        int regb = 0;
+        {
+            double ms = 0;
+            long long n = 0;
+            timing(MPS_K_PASS_B, &ms, &n, false);
+            if (n > 0 && ms / n < best[MPS_K_PASS_B]) regb |= 1;
+            ms = 0;
+            n = 0;
+            timing(MPS_K_PASS_C, &ms, &n, false);
+            if (n > 0 && ms / n < best[MPS_K_PASS_C]) regb |= 2;
+            timing(0, nullptr, nullptr, true);
+        }
+        reg_bound = regb;
         load_fluid(true);  // back to the snapshot: tuning leaves no trace in the results
         steps = steps0;
         timing_on = timing0;
         invalidate_graph();
         CK(cudaStreamSynchronize(stream));
         tuned_cache_put(tune_key(), Tuned{{blk[0], blk[1], blk[2], blk[3], blk[4], blk[5]},
-                                          stage_mode, batch_a});
+                                          stage_mode, batch_a, reg_bound});
         if (chosen)
             for (int k = 0; k < MPS_K_COUNT; ++k) chosen[k] = blk[k];
     }

@@ -270,12 +270,14 @@ class MPSBatch:
 
     def autotune(self, trial_steps: int = 3) -> dict:
         """Pick the fastest shapes per kernel group (state restored afterwards): block
-        sizes, and where VscTrm's walk reads its candidates (key "staging")."""
+        sizes, where VscTrm's walk reads its candidates (key "staging"), its candidates per
+        batch, and the register bound of passes B and C (key "register_bound", bits)."""
         out = (C.c_int32 * len(L.KERNEL_GROUPS))()
         check(lib().mps_autotune(self._h, int(trial_steps), out), "mps_autotune")
         d = dict(zip(L.KERNEL_GROUPS, out[:]))
         d["staging"] = self.get_option(L.OPT_STAGING)
         d["candidate_batch"] = self.get_option(L.OPT_CANDIDATE_BATCH)
+        d["register_bound"] = self.get_option(L.OPT_REGISTER_BOUND)
         return d
 
     def integrals(self, scene: int = 0) -> np.ndarray:

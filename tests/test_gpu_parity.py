@@ -175,8 +175,8 @@ def test_state_roundtrip_and_errors():
 
 @pytest.mark.parametrize("prec", [F32, F64])
 def test_autotune_changes_no_result(prec):
-    """Tuning tries every candidate of every knob (VscTrm's staging mode and block size, the
-    other passes' block sizes) on the handle's own state and restores it: the steps after
+    """Tuning tries every candidate of every knob (VscTrm's staging mode, candidate batch and
+    block size, the other passes' block sizes and register bounds) on the handle's own state and restores it: the steps after
     it equal the oracle's. Then each knob is forced to every value it can take, and the
     result is still the oracle's."""
     g, o, _, _ = _pair("dambreak_l0.02_6k", prec, diag=False)
@@ -184,6 +184,7 @@ def test_autotune_changes_no_result(prec):
     chosen = g.autotune(2)
     assert chosen["pass_a"] in (64, 128) and chosen["staging"] in (0, 1, 2)
     assert chosen["candidate_batch"] in (2, 4, 8)
+    assert chosen["register_bound"] in (0, 1, 2, 3)
     for k in ("pass_b", "pass_c", "gen_cull"):
         assert chosen[k] in (32, 64, 96, 128)
     assert g.counters()["steps"] == 2
@@ -204,6 +205,11 @@ def test_autotune_changes_no_result(prec):
         g.step(1)
         o.step(1)
         _assert_same_state(g.state(), o.state(), ("batch", nb))
+    for rb in (1, 2, 3, 0):
+        g.set_option(L.OPT_REGISTER_BOUND, rb)
+        g.step(1)
+        o.step(1)
+        _assert_same_state(g.state(), o.state(), ("register bound", rb))
     g.close()
 
 
@@ -213,6 +219,7 @@ def test_tuned_shapes_carry_over_to_a_new_handle_of_the_same_class():
     h = MPS(p, *args)
     assert h.get_option(L.OPT_STAGING) == chosen["staging"]
     assert h.get_option(L.OPT_BLOCK) == chosen["pass_a"]
+    assert h.get_option(L.OPT_REGISTER_BOUND) == chosen["register_bound"]
     h.close()
     g.close()
 

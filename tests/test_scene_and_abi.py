@@ -36,6 +36,21 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(lib, s)
 
 
+def test_binding_constants_equal_the_header_enums():
+    """Every MPS_OPT_*, MPS_STAGE_* and MPS_K_* value the Python binding uses is the header's."""
+    txt = open(HEADER).read()
+    enums = {m[0]: int(m[1]) for m in re.findall(r"\b(MPS_(?:OPT|STAGE|K)_\w+)\s*=\s*(\d+)", txt)}
+    assert len(enums) >= 20
+    for name, value in enums.items():
+        py = name[len("MPS_"):]
+        if name == "MPS_K_COUNT":
+            assert len(L.KERNEL_GROUPS) == value
+        elif hasattr(L, py):
+            assert getattr(L, py) == value, name
+    for name in ("MPS_OPT_REGISTER_BOUND", "MPS_OPT_CANDIDATE_BATCH", "MPS_OPT_STAGING"):
+        assert getattr(L, name[len("MPS_"):]) == enums[name]
+
+
 def test_status_strings():
     lib = L.lib()
     for code in range(9):

@@ -165,10 +165,10 @@ enum {
                                 global memory. Results never depend on it.               */
     MPS_OPT_CANDIDATE_BATCH = 9, /* VscTrm's candidates loaded together per particle: 2, 4
                                 or 8 (0 = 4). Results never depend on it.                */
-    MPS_OPT_REGISTER_BOUND = 10 /* bit 0: ChkCol/MkPrs, bit 1: PrsGrdTrm at their alternate
-                                register bound per thread (more or fewer resident blocks
-                                per SM; 0 = both at the default). Results never depend
-                                on it.                                                    */
+    MPS_OPT_REGISTER_BOUND = 10 /* bit 0: ChkCol/MkPrs, bit 1: PrsGrdTrm, bit 2: VscTrm
+                                (walking global memory) at their alternate register bound
+                                per thread (more or fewer resident blocks per SM; 0 = all
+                                at the default). Results never depend on it.              */
 };
 
 /* MPS_OPT_STAGING. GLOBAL: each particle walks its fine cells through L1. POSITIONS: a block
@@ -326,8 +326,8 @@ int mps_get_timing(mps_handle* h, int32_t kernel, double* total_ms, int64_t* lau
  * timed over `trial_steps` steps with CUDA events and the fastest kept, per kernel group:
  * VscTrm's candidates in flight (MPS_OPT_CANDIDATE_BATCH: 2, 4, 8), threads per block (128,
  * 64) and candidate source (MPS_OPT_STAGING); ChkCol/MkPrs, PrsGrdTrm and the mirror
- * generation with 128, 96, 64 or 32 threads per block; then ChkCol/MkPrs and PrsGrdTrm at
- * their alternate register bound (MPS_OPT_REGISTER_BOUND). The state is restored afterwards,
+ * generation with 128, 96, 64 or 32 threads per block; then ChkCol/MkPrs, PrsGrdTrm and
+ * VscTrm at their alternate register bound (MPS_OPT_REGISTER_BOUND). The state is restored afterwards,
  * so tuning changes no result (no kernel's arithmetic depends on these shapes).
  * chosen[MPS_K_COUNT] receives the block sizes (may be NULL); mps_get_option reads the
  * other knobs. The choice is kept for the process: a handle created later with the same

@@ -203,8 +203,8 @@ int mps_set_option(mps_handle* h, int32_t opt, int32_t value) {
                 s.invalidate_graph();
                 break;
             case MPS_OPT_REGISTER_BOUND:
-                if (value < 0 || value > 3)
-                    throw ApiError(MPS_ERR_ARG, "register bound must lie in [0, 3]");
+                if (value < 0 || value > 7)
+                    throw ApiError(MPS_ERR_ARG, "register bound must lie in [0, 7]");
                 s.reg_bound = value;
                 s.invalidate_graph();
                 break;

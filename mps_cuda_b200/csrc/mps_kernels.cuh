@@ -481,16 +481,20 @@ __device__ __forceinline__ size_t list_at(int s, int k, int K) {
 // take two registers each (at the FP32 bound the FP64 kernels spill).
 template <class R> constexpr int min_blocks(int f32) { return sizeof(R) == 8 ? f32 / 2 : f32; }
 
-// Two register bounds each for passes B and C (MPS_OPT_REGISTER_BOUND, chosen by the
-// autotuner); which is faster depends on the grid's size and the precision. Pass B: the
-// registers the compiler wants (FP32 64, FP64 96), or about one more resident block per SM
-// with a few spills (FP32 56, FP64 80). Pass C: 8 blocks per SM (FP32 64 registers without
-// spills, FP64 64 with about 200 bytes of spills), or FP32 10 blocks (48) and FP64 4 blocks
-// (122, no spills). Measured with CUDA events: at 6.1M particles in FP32 the alternate bounds
-// take pass B from 2.34 to 2.09 ms and pass C from 1.18 to 1.11 ms; in FP64 the spill-free
-// pass C is 9 % faster at 48 000 particles and 10 % slower at 384 000.
+// Two register bounds each for passes A, B and C (MPS_OPT_REGISTER_BOUND, chosen by the
+// autotuner); which is faster depends on the grid's size, the precision and pass A's
+// candidate batch. Passes A and B: 8 resident blocks of 128 threads per SM in FP32 (64
+// registers) and 5 in FP64 (up to 102), or one block more (FP32 56 registers, FP64 80) with
+// a few spills. Pass C: 8 blocks per SM (FP32 64 registers without spills, FP64 64 with
+// about 200 bytes of spills), or FP32 10 blocks (48) and FP64 4 blocks (122, no spills).
+// Measured with CUDA events at 6.1M particles in FP32, the alternate bounds take pass A
+// from 3.77 to 3.72 ms, pass B from 2.34 to 2.09 ms and pass C from 1.18 to 1.11 ms; in FP64
+// the spill-free pass C is 9 % faster at 48 000 particles and 10 % slower at 384 000.
+template <class R> constexpr int pass_a_blocks(bool alt) {
+    return sizeof(R) == 8 ? (alt ? 6 : 5) : (alt ? 9 : 8);
+}
 template <class R> constexpr int pass_b_blocks(bool alt) {
-    return alt ? (sizeof(R) == 8 ? 6 : 9) : 1;
+    return sizeof(R) == 8 ? (alt ? 6 : 5) : (alt ? 9 : 8);
 }
 template <class R> constexpr int pass_c_blocks(bool alt, bool corr) {
     return corr ? min_blocks<R>(6) : alt ? (sizeof(R) == 8 ? 4 : 10) : 8;
@@ -900,8 +904,9 @@ __device__ __forceinline__ void pass_a_unlisted(const PassArgs<R, RN>& a, int s,
 // pass A: VscTrm (kernel.cu:1013-1119) + UpPcl1/ChkPcl (kernel.cu:1138-1149, 481-513), each
 // particle walking its candidates in global memory (posf through L1).
 // TAPE (recorded rollouts): also keeps the list length and the velocity before the clamp.
-template <class R, class RN, bool DIAG, bool TAPE = false, int NB = 4>
-__global__ void __launch_bounds__(128) k_pass_a(const __grid_constant__ PassArgs<R, RN> a) {
+template <class R, class RN, bool DIAG, bool TAPE = false, int NB = 4, bool ALT = false>
+__global__ void __launch_bounds__(128, pass_a_blocks<R>(ALT))
+    k_pass_a(const __grid_constant__ PassArgs<R, RN> a) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= a.nF) return;
     const int nalive = __ldg(a.cs + a.dead);

@@ -273,7 +273,7 @@ struct SolverBase {
     int stage_mode = MPS_STAGE_GLOBAL;  // pass A's candidate source (MPS_OPT_STAGING)
     int stage_cap = 0;                  // candidates staged per block (MPS_OPT_STAGE_CAPACITY)
     int batch_a = 4;                    // VscTrm's candidates in flight (MPS_OPT_CANDIDATE_BATCH)
-    int reg_bound = 0;                  // passes B, C at their alternate register bound (bits 0, 1)
+    int reg_bound = 0;                  // passes B, C, A at their alternate register bound (bits 0-2)
     long long steps = 0;
     long long launches = 0;       // kernels launched (graph replays included)
     long long body_launches = 0;  // kernels of one captured step
@@ -817,20 +817,28 @@ template <class R, class RN> class Solver final : public SolverBase {
         else launch_pass_a_staged_v<D, false>(ba);
     }
 
+    // pass A walking global memory, at the handle's candidate batch
+    template <bool D, bool ALT> void launch_pass_a(int ba) {
+        if (batch_a == 2)
+            k_pass_a<R, RN, D, false, 2, ALT><<<blocks(nF, ba), ba, 0, stream>>>(args(M1, mcs1));
+        else if (batch_a == 8)
+            k_pass_a<R, RN, D, false, 8, ALT><<<blocks(nF, ba), ba, 0, stream>>>(args(M1, mcs1));
+        else
+            k_pass_a<R, RN, D, false, 4, ALT><<<blocks(nF, ba), ba, 0, stream>>>(args(M1, mcs1));
+    }
+
     template <bool D> void fused_body() {
         const int ba = blk[MPS_K_PASS_A], bb = blk[MPS_K_PASS_B], bc = blk[MPS_K_PASS_C],
                   bg = blk[MPS_K_GEN];
         // pass A: VscTrm + UpPcl1
         {
             Scope t(this, MPS_K_PASS_A);
-            if (stage_mode == MPS_STAGE_GLOBAL && batch_a == 2)
-                k_pass_a<R, RN, D, false, 2><<<blocks(nF, ba), ba, 0, stream>>>(args(M1, mcs1));
-            else if (stage_mode == MPS_STAGE_GLOBAL && batch_a == 8)
-                k_pass_a<R, RN, D, false, 8><<<blocks(nF, ba), ba, 0, stream>>>(args(M1, mcs1));
-            else if (stage_mode == MPS_STAGE_GLOBAL)
-                k_pass_a<R, RN, D><<<blocks(nF, ba), ba, 0, stream>>>(args(M1, mcs1));
-            else
+            if (stage_mode != MPS_STAGE_GLOBAL)
                 launch_pass_a_staged<D>(ba);
+            else if (reg_bound & 4)
+                launch_pass_a<D, true>(ba);
+            else
+                launch_pass_a<D, false>(ba);
             KL();
         }
         // MkBkt on x* (kernel.cu:1917); the rebuild at kernel.cu:1921 would give the same lists
@@ -906,7 +914,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     //   pass A (VscTrm): candidates in flight (2, 4, 8) and 128 or 64 threads per block
     //                    for the walk through L1, and the staged walk at 128 threads;
     //   passes B, C and mirror generation: 128, 96, 64 or 32 threads per block;
-    //   then passes B and C at their alternate register bound, with the chosen block sizes.
+    //   then passes B, C and A at their alternate register bound, with the chosen shapes.
     // All groups are timed in the same trial steps (they are separate kernels). The state is
     // restored afterwards, and the choice is kept for later handles of the same precision
     // and size class in this process (tuned_cache).
@@ -962,8 +970,8 @@ template <class R, class RN> class Solver final : public SolverBase {
         blk[MPS_K_PASS_A] = bestb[MPS_K_PASS_A];
         stage_mode = best_stage;
         batch_a = best_batch;
-        // the alternate register bounds of passes B and C, at the chosen shapes
-        reg_bound = 3;
+        // the alternate register bounds of passes B, C and A, at the chosen shapes
+        reg_bound = 7;
         step(trial);
         int regb = 0;
         {
@@ -975,6 +983,10 @@ template <class R, class RN> class Solver final : public SolverBase {
             n = 0;
             timing(MPS_K_PASS_C, &ms, &n, false);
             if (n > 0 && ms / n < best[MPS_K_PASS_C]) regb |= 2;
+            ms = 0;
+            n = 0;
+            timing(MPS_K_PASS_A, &ms, &n, false);
+            if (stage_mode == MPS_STAGE_GLOBAL && n > 0 && ms / n < best[MPS_K_PASS_A]) regb |= 4;
             timing(0, nullptr, nullptr, true);
         }
         reg_bound = regb;

@@ -271,7 +271,7 @@ class MPSBatch:
     def autotune(self, trial_steps: int = 3) -> dict:
         """Pick the fastest shapes per kernel group (state restored afterwards): block
         sizes, where VscTrm's walk reads its candidates (key "staging"), its candidates per
-        batch, and the register bound of passes B and C (key "register_bound", bits)."""
+        batch, and the register bound of passes B, C and A (key "register_bound", bits 0-2)."""
         out = (C.c_int32 * len(L.KERNEL_GROUPS))()
         check(lib().mps_autotune(self._h, int(trial_steps), out), "mps_autotune")
         d = dict(zip(L.KERNEL_GROUPS, out[:]))

@@ -383,6 +383,10 @@ def run_ours(args, world, rank, local):
 
     # ---- timed region: K steps, L2 flushed between steps (outside the events) ----------
     K = args.steps
+    # the state the timed steps start from: the per-kernel split below replays the same
+    # simulated steps (a dam break's steps grow slower as the column collapses, so later
+    # steps would not describe the timed ones)
+    start = g.state()
     e0 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     e1 = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     l0 = g.counters()["kernel_launches"]
@@ -409,7 +413,8 @@ def run_ours(args, world, rank, local):
     value = world * nf * K / (dev_ms_max / 1e3)
     cnt = g.counters()
 
-    # ---- per-kernel device times (CUDA events on the solver's stream), same workload ---
+    # ---- per-kernel device times (CUDA events on the solver's stream), same steps -----
+    g.set_state(**start)
     g.set_option(L.OPT_TIMING, 1)
     g.timing(reset=True)
     with torch.cuda.stream(stream):
@@ -437,18 +442,24 @@ def run_ours(args, world, rank, local):
                 "ms_per_launch": groups[dom]["ms_per_launch"]}
 
     # ---- companion compute roofline: the passes' pair arithmetic against the device's
-    # own measured FMA / sqrt / division rates, from one more step run with the device
-    # counting its work (after the timed region) --------------------------------------
+    # own measured FMA / sqrt / division rates, the device counting its work in four
+    # steps spread over the timed steps (replayed from their start) ---------------------
     compute = None
     if not args.no_compute:
         from mps_cuda_b200 import measure_arith
         ar = measure_arith()
-        w0 = g.work()
-        g.set_option(L.OPT_DIAG, 1)
-        g.step(1)
-        g.set_option(L.OPT_DIAG, 0)
-        w1 = g.work()
-        ops = pair_arith({k: w1[k] - w0[k] for k in w1}, g.diag())
+        g.set_state(**start)
+        samples = []
+        for i in range(4):
+            g.step(max(K // 4 - 1, 0))
+            w0 = g.work()
+            g.set_option(L.OPT_DIAG, 1)
+            g.step(1)
+            g.set_option(L.OPT_DIAG, 0)
+            w1 = g.work()
+            samples.append(pair_arith({k: w1[k] - w0[k] for k in w1}, g.diag()))
+        ops = {k_: tuple(float(np.mean([sm[k_][j] for sm in samples])) for j in range(3))
+               for k_ in samples[0]}
         ia = issue_active(args.workload, args.precision)
         compute = {"arith_peaks": ar, "issue_active_source": "profiles/issue_active.json (ncu)",
                    "groups": {}}
@@ -469,7 +480,7 @@ def run_ours(args, world, rank, local):
         # acc is ChkCol's scratch and zero between steps (kernel.cu:1146, 1826), and the
         # pressures a step starts from only reach the first mirror generation's PrsM, which
         # no later term reads (VscTrm, ChkCol and MkPrs use mirror positions only).
-        st0 = g.state()
+        st0 = start  # the same simulated steps as the timed region
         ins, outs = ("typ", "pos", "vel", "pav"), ("typ", "pos", "vel", "prs", "pav")
 
         def pinned_like(keys):

@@ -286,7 +286,12 @@ int mps_set_wall_motion(mps_handle* h, int32_t type, const double center[3],
 
 /* ---- time stepping ---------------------------------------------------------------- */
 
-/* Advance every scene by `nsteps` steps of the loop body kernel.cu:1904-1941. */
+/* Advance every scene by `nsteps` steps of the loop body kernel.cu:1904-1941. The end of a
+ * step (the next step's first mirror generation and the bucket builds of the new positions)
+ * is queued at the start of the next step, or before any call that reads the sorted state
+ * (mps_phase, mps_get_mirrors of generation 0 or 1, mps_get_integrals, mps_autotune,
+ * mps_adjoint_record); a state replaced with mps_set_state in between never builds it.
+ * Results are the same either way. */
 int mps_step(mps_handle* h, int32_t nsteps);
 /* Run one method of the reference's step on its own (MPS_PHASE_*). */
 int mps_phase(mps_handle* h, int32_t phase);

@@ -1642,7 +1642,7 @@ __global__ void k_surface_edge(const SceneDev<R, RN>* scs, int nscene, int nW, W
 // ---------------------------------------------------------------------------------------
 // state transfer between id order (host layout) and slot order
 // ---------------------------------------------------------------------------------------
-template <class R> struct IdState {  // SoA, id order, n = all particles
+template <class R> struct IdState {  // SoA, id order, n = all particles; a null array is skipped
     int n;
     R* pos; R* vel; R* acc; R* prs; R* pav; int8_t* typ;
     int* cell;  // bucket index ib of the current position, -1 for GST
@@ -1700,13 +1700,21 @@ __global__ void k_store_fluid(IdState<R> st, const SceneDev<R, RN>* scs, int nsc
         st.cell[id] = typ[s] == kFLD ? local_cell(sc, pos[s].x, pos[s].y, pos[s].z) : -1;
     }
     const size_t n = st.n;
-    V4<R> p = pos[s], v = vel[s], a = acc[s];
-    st.pos[id] = p.x; st.pos[n + id] = p.y; st.pos[2 * n + id] = p.z;
-    st.vel[id] = v.x; st.vel[n + id] = v.y; st.vel[2 * n + id] = v.z;
-    st.acc[id] = a.x; st.acc[n + id] = a.y; st.acc[2 * n + id] = a.z;
-    st.prs[id] = prs[s];
-    st.pav[id] = pav[s];
-    st.typ[id] = typ[s];
+    if (st.pos) {
+        const V4<R> p = pos[s];
+        st.pos[id] = p.x; st.pos[n + id] = p.y; st.pos[2 * n + id] = p.z;
+    }
+    if (st.vel) {
+        const V4<R> v = vel[s];
+        st.vel[id] = v.x; st.vel[n + id] = v.y; st.vel[2 * n + id] = v.z;
+    }
+    if (st.acc) {
+        const V4<R> a = acc[s];
+        st.acc[id] = a.x; st.acc[n + id] = a.y; st.acc[2 * n + id] = a.z;
+    }
+    if (st.prs) st.prs[id] = prs[s];
+    if (st.pav) st.pav[id] = pav[s];
+    if (st.typ) st.typ[id] = typ[s];
 }
 
 template <class R, class RN>
@@ -1721,13 +1729,18 @@ __global__ void k_store_walls(IdState<R> st, const SceneDev<R, RN>* scs, int nsc
         st.cell[id] = local_cell(sc, pos[w].x, pos[w].y, pos[w].z);
     }
     const size_t n = st.n;
-    V4<R> p = pos[w], v = vel[w];
-    st.pos[id] = p.x; st.pos[n + id] = p.y; st.pos[2 * n + id] = p.z;
-    st.vel[id] = v.x; st.vel[n + id] = v.y; st.vel[2 * n + id] = v.z;
-    st.acc[id] = R(0); st.acc[n + id] = R(0); st.acc[2 * n + id] = R(0);
-    st.prs[id] = R(0);
-    st.pav[id] = R(0);
-    st.typ[id] = wtyp[w];
+    if (st.pos) {
+        const V4<R> p = pos[w];
+        st.pos[id] = p.x; st.pos[n + id] = p.y; st.pos[2 * n + id] = p.z;
+    }
+    if (st.vel) {
+        const V4<R> v = vel[w];
+        st.vel[id] = v.x; st.vel[n + id] = v.y; st.vel[2 * n + id] = v.z;
+    }
+    if (st.acc) { st.acc[id] = R(0); st.acc[n + id] = R(0); st.acc[2 * n + id] = R(0); }
+    if (st.prs) st.prs[id] = R(0);
+    if (st.pav) st.pav[id] = R(0);
+    if (st.typ) st.typ[id] = wtyp[w];
 }
 
 // per-scene integrals over the listed fluid slots [cs[fbase], cs[fbase + 27 nbxyz])

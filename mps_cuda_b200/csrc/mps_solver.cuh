@@ -276,7 +276,8 @@ struct SolverBase {
     int reg_bound = 0;                  // passes B, C, A at their alternate register bound (bits 0-2)
     long long steps = 0;
     long long launches = 0;       // kernels launched (graph replays included)
-    long long body_launches = 0;  // kernels of one captured step
+    long long head_launches = 0;  // kernels of one captured step up to PrsGrdTrm
+    long long tail_launches = 0;  // kernels of one captured step end (mirrors, bucket builds)
     bool timing_on = false;
     double t_ms[MPS_K_COUNT] = {};
     long long t_n[MPS_K_COUNT] = {};
@@ -380,8 +381,22 @@ template <class R, class RN> class Solver final : public SolverBase {
     int nbK = kListCap;                    // list capacity in use (MPS_OPT_LIST_CAPACITY)
     std::vector<int> fluid_ids, wall_ids;
     bool lists_valid = false, sorted = false, m1_valid = false, acc_dirty = false;
-    cudaGraphExec_t gexec = nullptr;
+    // Captured graphs of a step's body (passes A to C, moving walls) and of a step's end (the
+    // next step's mirrors and bucket builds), one per buffer the sorted state starts in: each
+    // holds one fluid bucket build, which moves the state from S to S2, so a graph's baked
+    // pointers fit only the buffer it was captured from. A replay swaps S and S2 on the host
+    // as the captured build did.
+    cudaGraphExec_t gx_head[2] = {nullptr, nullptr};
+    cudaGraphExec_t gx_tail[2] = {nullptr, nullptr};
+    int swaps_head = 0, swaps_tail = 0;  // fluid bucket builds in each
+    const void* sbuf0 = nullptr;          // S.pos at allocation: buffer 0
+    int swap_count = 0;                   // fluid bucket builds issued on the host
     bool gexec_diag = false;
+    // The end of the latest step (the next step's first mirror generation and the bucket
+    // build of x^{n+1}) has not run yet: the state lives in the scratch arrays t_* in the
+    // slot order of S. It runs when the next step starts or when something reads the sorted
+    // state, so a state replaced in between (mps_set_state) wastes no build.
+    bool tail_pending = false;
     // CUDA events bracketing kernel groups when timing_on
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
@@ -440,7 +455,10 @@ template <class R, class RN> class Solver final : public SolverBase {
     }
 
     ~Solver() override {
-        if (gexec) cudaGraphExecDestroy(gexec);
+        for (int b = 0; b < 2; ++b) {
+            if (gx_head[b]) cudaGraphExecDestroy(gx_head[b]);
+            if (gx_tail[b]) cudaGraphExecDestroy(gx_tail[b]);
+        }
         for (auto& pe : ev_pending) {
             cudaEventDestroy(pe.second.first);
             cudaEventDestroy(pe.second.second);
@@ -574,6 +592,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         for (FluidBuf<R>* b : {&S, &S2}) {
             b->pos = ar.template get<V4<R>>(F);
             b->vel = ar.template get<V4<R>>(F);
+            if (b == &S) sbuf0 = b->pos;
             b->acc = ar.template get<V4<R>>(F);
             b->prs = ar.template get<R>(F);
             b->pav = ar.template get<R>(F);
@@ -697,6 +716,7 @@ template <class R, class RN> class Solver final : public SolverBase {
             KL();
         }
         std::swap(S, S2);
+        ++swap_count;
         posf_stale = false;
     }
 
@@ -876,6 +896,12 @@ template <class R, class RN> class Solver final : public SolverBase {
         }
         // walls that move take their place at the new time before the next step's mirrors
         if (motion_on) move_walls();
+    }
+
+    // the end of a step: the next step's first mirror generation at x^{n+1}, then the bucket
+    // builds of x^{n+1} and of those mirrors
+    void step_tail() {
+        const int bg = blk[MPS_K_GEN];
         reset_raw();
         {
             Scope t(this, MPS_K_GEN);
@@ -886,6 +912,13 @@ template <class R, class RN> class Solver final : public SolverBase {
         }
         bin_fluid(t_pos, t_vel, nullptr, t_prs, S.pav, S.pid, t_typ);
         bin_mirrors(M1, mcs1);
+    }
+
+    // runs the pending end of the latest step, if any (before reading the sorted state)
+    void finish_tail() {
+        if (!tail_pending) return;
+        step_tail();
+        tail_pending = false;
     }
 
     void prepare_fused() {
@@ -906,6 +939,27 @@ template <class R, class RN> class Solver final : public SolverBase {
         }
     }
 
+    // one instantiated CUDA graph of `body`'s launches; `nl` receives their count
+    template <class F> void capture(cudaGraphExec_t& ge, long long& nl, int& nswap, F&& body) {
+        cudaGraph_t g;
+        const long long l0 = launches;
+        const int s0 = swap_count;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            body();
+        } catch (...) {
+            cudaStreamEndCapture(stream, &g);
+            throw;
+        }
+        CK(cudaStreamEndCapture(stream, &g));
+        nl = launches - l0;
+        nswap = swap_count - s0;
+        launches = l0;  // captured, not yet run
+        cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+        cudaGraphDestroy(g);
+        CK(e);
+    }
+
     void run_body() {
         if (diag_on) fused_body<true>(); else fused_body<false>();
     }
@@ -919,6 +973,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     // restored afterwards, and the choice is kept for later handles of the same precision
     // and size class in this process (tuned_cache).
     void autotune(int trial, int32_t* chosen) override {
+        finish_tail();
         struct CandA { int blk, stage, batch; };
         const CandA cand_a[] = {{128, MPS_STAGE_GLOBAL, 4}, {64, MPS_STAGE_GLOBAL, 4},
                                 {128, MPS_STAGE_GLOBAL, 2}, {64, MPS_STAGE_GLOBAL, 2},
@@ -1017,50 +1072,55 @@ template <class R, class RN> class Solver final : public SolverBase {
     }
 
     void invalidate_graph() override {
-        if (gexec) cudaGraphExecDestroy(gexec);
-        gexec = nullptr;
+        for (int b = 0; b < 2; ++b) {
+            if (gx_head[b]) cudaGraphExecDestroy(gx_head[b]);
+            if (gx_tail[b]) cudaGraphExecDestroy(gx_tail[b]);
+            gx_head[b] = gx_tail[b] = nullptr;
+        }
     }
 
+    // Launches the graph of `body` for the buffer the sorted state is in, capturing it first
+    // if needed (the capture runs the host side of `body`, its swaps included); a replay
+    // repeats the captured swaps on the host.
+    template <class F>
+    void run_graph(cudaGraphExec_t* gx, long long& nl, int& nswap, F&& body) {
+        const int b = S.pos == sbuf0 ? 0 : 1;
+        if (!gx[b]) {
+            capture(gx[b], nl, nswap, body);
+        } else {
+            for (int k = 0; k < nswap; ++k) std::swap(S, S2);
+            swap_count += nswap;
+            if (nswap) posf_stale = false;
+        }
+        CK(cudaGraphLaunch(gx[b], stream));
+        launches += nl;
+    }
+
+    // A step is its body (passes A to C) preceded by the end of the step before it, or by a
+    // full bucket build and mirror generation when the state was set or changed since.
     void step(int n) override {
         if (n <= 0) return;
-        int done = 0;
-        if (!(lists_valid && sorted && m1_valid) || acc_dirty) {
-            prepare_fused();
-            run_body();
-            ++done;
-        }
-        if (graph_on && !timing_on && n - done > 0) {
-            if (gexec && gexec_diag != diag_on) invalidate_graph();
-            if (!gexec) {
-                cudaGraph_t g;
-                const long long l0 = launches;
-                CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-                try {
-                    run_body();
-                } catch (...) {
-                    cudaStreamEndCapture(stream, &g);
-                    throw;
-                }
-                CK(cudaStreamEndCapture(stream, &g));
-                body_launches = launches - l0;
-                launches = l0;  // captured, not yet run
-                cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
-                cudaGraphDestroy(g);
-                CK(e);
-                gexec_diag = diag_on;
+        const bool use_graph = graph_on && !timing_on;
+        if (gexec_diag != diag_on) invalidate_graph();
+        gexec_diag = diag_on;
+        for (int k = 0; k < n; ++k) {
+            if (tail_pending) {
+                if (use_graph) run_graph(gx_tail, tail_launches, swaps_tail, [&] { step_tail(); });
+                else step_tail();
+                tail_pending = false;
+            } else if (!(lists_valid && sorted && m1_valid) || acc_dirty) {
+                prepare_fused();
             }
-            for (; done < n; ++done) {
-                CK(cudaGraphLaunch(gexec, stream));
-                launches += body_launches;
-            }
-        } else {
-            for (; done < n; ++done) run_body();
+            if (use_graph) run_graph(gx_head, head_launches, swaps_head, [&] { run_body(); });
+            else run_body();
+            tail_pending = true;
+            lists_valid = sorted = m1_valid = true;  // as the pending end will leave them
         }
         steps += n;
-        lists_valid = sorted = m1_valid = true;
     }
 
     void phase(int ph) override {
+        finish_tail();
         PassArgs<R, RN> a = args(M1, mcs1);
         const int gb = blocks(nF, block);
         auto need_lists = [&]() {
@@ -1158,21 +1218,43 @@ template <class R, class RN> class Solver final : public SolverBase {
         KL();
         lists_valid = sorted = m1_valid = false;
         acc_dirty = use_acc;
+        tail_pending = false;  // the loaded state replaces what the latest step left
     }
 
-    void store_all() {
-        k_store_fluid<R, RN><<<blocks(nF, 256), 256, 0, stream>>>(io, d_sc, nscene, nF, S.pos, S.vel,
-                                                                  S.acc, S.prs, S.pav, S.pid, S.typ);
+    // the state in id order into io; with a step's end pending, from the arrays pass C left
+    // (in S's slot order; acc is zero between steps in both). `mask` (kIo* bits) selects the
+    // arrays; the bucket index of each particle (io.cell) comes with kIoCell.
+    static constexpr int kIoPos = 1, kIoVel = 2, kIoAcc = 4, kIoPrs = 8, kIoPav = 16,
+                         kIoTyp = 32, kIoCell = 64, kIoAll = 127;
+    void store_all(int mask = kIoAll) {
+        IdState<R> st = io;
+        if (!(mask & kIoPos)) st.pos = nullptr;
+        if (!(mask & kIoVel)) st.vel = nullptr;
+        if (!(mask & kIoAcc)) st.acc = nullptr;
+        if (!(mask & kIoPrs)) st.prs = nullptr;
+        if (!(mask & kIoPav)) st.pav = nullptr;
+        if (!(mask & kIoTyp)) st.typ = nullptr;
+        if (!(mask & kIoCell)) st.cell = nullptr;
+        if (!(mask & kIoAll)) return;
+        if (tail_pending)
+            k_store_fluid<R, RN><<<blocks(nF, 256), 256, 0, stream>>>(st, d_sc, nscene, nF, t_pos,
+                                                                      t_vel, S.acc, t_prs, S.pav,
+                                                                      S.pid, t_typ);
+        else
+            k_store_fluid<R, RN><<<blocks(nF, 256), 256, 0, stream>>>(st, d_sc, nscene, nF, S.pos,
+                                                                      S.vel, S.acc, S.prs, S.pav,
+                                                                      S.pid, S.typ);
         KL();
         if (nW > 0) {
-            k_store_walls<R, RN><<<blocks(nW, 256), 256, 0, stream>>>(io, d_sc, nscene, nW, w_pos,
+            k_store_walls<R, RN><<<blocks(nW, 256), 256, 0, stream>>>(st, d_sc, nscene, nW, w_pos,
                                                                       w_vel, w_id, w_typ);
             KL();
         }
     }
 
     void get_state(int8_t* typ, void* pos, void* vel, void* acc, void* prs, void* pav) override {
-        store_all();
+        store_all((typ ? kIoTyp : 0) | (pos ? kIoPos : 0) | (vel ? kIoVel : 0) |
+                  (acc ? kIoAcc : 0) | (prs ? kIoPrs : 0) | (pav ? kIoPav : 0));
         const size_t n3 = 3 * size_t(nT) * sizeof(R), n1 = size_t(nT) * sizeof(R);
         if (typ) CK(cudaMemcpyAsync(typ, io.typ, nT, cudaMemcpyDeviceToHost, stream));
         if (pos) CK(cudaMemcpyAsync(pos, io.pos, n3, cudaMemcpyDeviceToHost, stream));
@@ -1186,7 +1268,8 @@ template <class R, class RN> class Solver final : public SolverBase {
     void set_state(const int8_t* typ, const void* pos, const void* vel, const void* acc,
                    const void* prs, const void* pav) override {
         // start from the current state so that omitted arrays keep their values
-        store_all();
+        store_all((typ ? 0 : kIoTyp) | (pos ? 0 : kIoPos) | (vel ? 0 : kIoVel) |
+                  (acc ? 0 : kIoAcc) | (prs ? 0 : kIoPrs) | (pav ? 0 : kIoPav));
         const size_t n3 = 3 * size_t(nT) * sizeof(R), n1 = size_t(nT) * sizeof(R);
         if (typ) CK(cudaMemcpyAsync(io.typ, typ, nT, cudaMemcpyHostToDevice, stream));
         if (pos) CK(cudaMemcpyAsync(io.pos, pos, n3, cudaMemcpyHostToDevice, stream));
@@ -1245,6 +1328,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     }
 
     int get_mirrors(int which, int cp, int32_t* slot, void* pos, void* prs) override {
+        if (which != 2) finish_tail();  // the raw list and M1 are the step end's generation
         int n = 0;
         const MirrorBuf<R>* b = which == 2 ? &M2 : (which == 1 ? &M1 : &U);
         if (which == 0) {
@@ -1304,7 +1388,8 @@ template <class R, class RN> class Solver final : public SolverBase {
         CK(cudaMemcpyAsync(&a1, mcs1 + dead(), sizeof(int), cudaMemcpyDeviceToHost, stream));
         CK(cudaMemcpyAsync(&a2, mcs2 + dead(), sizeof(int), cudaMemcpyDeviceToHost, stream));
         std::vector<int8_t> ty(std::max(nF, 1));
-        CK(cudaMemcpyAsync(ty.data(), S.typ, std::max(nF, 1), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(ty.data(), tail_pending ? t_typ : S.typ, std::max(nF, 1),
+                           cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
         for (int k = 0; k < nF; ++k) alive += ty[k] == kFLD;
         std::memset(o, 0, sizeof(*o));
@@ -1422,6 +1507,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     }
 
     void adjoint_record(int nsteps, int every) override {
+        finish_tail();
         if (grad_mode != MPS_GRAD_STANDARD)
             throw ApiError(MPS_ERR_UNSUPPORTED,
                            "the adjoint covers the default PrsGrdTrm only (MPS_GRAD_STANDARD)");
@@ -1602,6 +1688,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     }
 
     void integrals(int scene, double out[6]) override {
+        finish_tail();
         if (!lists_valid) mkbkt(acc_dirty);
         std::vector<double> init(6 * size_t(nscene), 0.0);
         for (int s = 0; s < nscene; ++s) init[6 * s + 4] = -1e300;

@@ -123,7 +123,8 @@ def test_rollout_100_steps_fp64():
     assert np.array_equal(g.diag()["ndens"], o.diag()["ndens"])
 
 
-def test_batched_scenes_equal_single_scenes():
+@pytest.mark.parametrize("prec", [F32, F32_N64])
+def test_batched_scenes_equal_single_scenes(prec):
     """Three scenes in one handle advance exactly like three separate oracles."""
     names = ["dambreak_l0.02_small", "dambreak_l0.02_small", "dambreak_l0.02_6k"]
     descs = []
@@ -132,7 +133,7 @@ def test_batched_scenes_equal_single_scenes():
         d = type(d)(**{**d.__dict__, "seed": d.seed + k})
         descs.append((d, dt))
     parts = [dambreak(d) for d, _ in descs]
-    params = [dambreak_params(d, dt=dt, precision=F32) for d, dt in descs]
+    params = [dambreak_params(d, dt=dt, precision=prec) for d, dt in descs]
     cat = lambda key: np.concatenate([p[key] for p in parts], axis=-1)
     counts = [p["typ"].shape[0] for p in parts]
     b = MPSBatch(params, cat("typ"), cat("pos").astype(np.float32), cat("vel").astype(np.float32),
@@ -224,7 +225,9 @@ def test_tuned_shapes_carry_over_to_a_new_handle_of_the_same_class():
     g.close()
 
 
-def test_batch_of_64_uneven_scenes_equals_separate_handles():
+def test_batch_of_64_uneven_scenes_equals_the_oracle():
+    """The bench's batched configuration (64 uneven scenes, FP32 state with FP64 number
+    density, graph replay): every scene equals its own oracle after four steps."""
     scenes = configs.batched_scenes()
     parts = [dambreak(d) for d, _ in scenes]
     params = [dambreak_params(d, dt=dt, precision=F32_N64) for d, dt in scenes]
@@ -236,13 +239,13 @@ def test_batch_of_64_uneven_scenes_equals_separate_handles():
     b.step(4)
     st = b.state()
     off = 0
-    for pp, pt, n in zip(params, parts, counts):
-        h = MPS(pp, pt["typ"], pt["pos"].astype(np.float32), pt["vel"].astype(np.float32),
-                pt["nrm"].astype(np.float32))
-        h.step(4)
+    for s, (pp, pt, n) in enumerate(zip(params, parts, counts)):
+        o = Oracle(params_from(pp), pt["typ"], pt["pos"].astype(np.float32),
+                   pt["vel"].astype(np.float32), pt["nrm"].astype(np.float32))
+        o.step(4)
         sub = {k: v[..., off:off + n] for k, v in st.items()}
-        _assert_same_state(sub, h.state())
-        h.close()
+        _assert_same_state(sub, o.state(), s)
+        o.close()
         off += n
 
 
@@ -285,3 +288,33 @@ def test_list_capacity_change_voids_a_recorded_rollout():
             g.set_option(L.OPT_LIST_CAPACITY, -1)
     finally:
         g.close()
+
+
+@pytest.mark.parametrize("graph", [0, 1])
+def test_reads_between_steps_change_nothing(graph):
+    """A step's end (the next step's mirrors and bucket builds) runs when the next step
+    starts or when something needs the sorted state. Reading the state, counters,
+    diagnostics or the step's second mirrors in between, or setting the state back to what
+    was read, leaves every later result equal to the oracle's."""
+    g, o, _, _ = _pair("dambreak_l0.02_6k", F32, diag=False)
+    h, _, _, _ = _pair("dambreak_l0.02_6k", F32, diag=False)
+    for x in (g, h):
+        x.set_option(L.OPT_GRAPH, graph)
+    for k in range(4):
+        g.step(1)
+        o.step(1)
+        st = g.state()
+        _assert_same_state(st, o.state(), ("state", k))
+        c = g.counters()
+        assert c["n_fluid_alive"] == int((o.state()["typ"] == L.FLD).sum())
+        _assert_same_mirrors(g.mirrors(2), o.mirrors(), ("m2", k))
+        if k == 2:
+            g.set_state(typ=st["typ"], pos=st["pos"], vel=st["vel"], pav=st["pav"])
+    h.step(4)
+    _assert_same_state(h.state(), o.state(), "stepped at once")
+    _assert_same_mirrors(g.mirrors(1), h.mirrors(1), "m1")
+    g.step(2)
+    o.step(2)
+    _assert_same_state(g.state(), o.state(), "after")
+    g.close()
+    h.close()

@@ -357,10 +357,11 @@ __device__ __forceinline__ void col_dens_walls_mirrors(const SceneDev<R, RN>& sc
                                                        R x, R y, R z, R ux, R uy, R uz,
                                                        const WallView<R>& wl,
                                                        const MirrorView<R>& m, bool skip, R& wx,
-                                                       R& wy, R& wz, RN& ni, int* cnt) {
+                                                       R& wy, R& wz, RN& ni, int* cnt,
+                                                       bool walls = true, bool mirrors = true) {
     const R inf = R(INFINITY);
     const R Bf = !skip ? inf : (COL && DENS ? sc.skip_rc : (DENS ? sc.skip_rp : sc.skip_rl));
-    if (COL) {
+    if (COL && walls) {
         for_rows(sc, wl.cs, c, skip ? sc.skip_rw : inf, [&](int j) {
             V4<R> q = ldg4(wl.pos + j);
             R dx = q.x - x, dy = q.y - y, dz = q.z - z;
@@ -372,6 +373,7 @@ __device__ __forceinline__ void col_dens_walls_mirrors(const SceneDev<R, RN>& sc
             }
         });
     }
+    if (!mirrors) return;
     for_rows(sc, m.cs, c, Bf, [&](int k) {
         V4<R> q = ldg4(m.pos + k);
         R dx = q.x - x, dy = q.y - y, dz = q.z - z;

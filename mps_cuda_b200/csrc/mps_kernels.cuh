@@ -525,6 +525,10 @@ template <class R, class RN> struct PassArgs {
     int* nbcnt;
     int nbK;
     const int8_t* near_wall;  // per bucket: a wall lies in the 27 buckets around it
+    // per bucket: a mirror of the view `m` lies in the 27 buckets around it (null: walk
+    // the mirrors everywhere). The wall and mirror walks visit only a particle's 27 buckets,
+    // so skipping them where these flags are clear changes no sum.
+    const int8_t* near_m;
     // recorded rollouts only: per slot the velocity before ChkPcl's clamp, w = slot state
     // (kTapeOk, kTapeClamped, kTapeDeleted, kTapeDead)
     V4<R>* tape_pre;
@@ -533,7 +537,8 @@ template <class R, class RN> struct PassArgs {
     const int* csr;
 };
 
-// near_wall flag of every bucket of every scene (walls are static: computed once)
+// near flag of every bucket of every scene: some item of the bucket table `wcs` (walls, or
+// the mirrors of one generation) lies in the 27 buckets around it
 template <class R, class RN>
 __global__ void k_near_wall(const SceneDev<R, RN>* scs, int nscene, const int* __restrict__ wcs,
                             int8_t* near_wall) {
@@ -562,6 +567,13 @@ __device__ __forceinline__ const SceneDev<R, RN>& scene_ref(const PassArgs<R, RN
 }
 
 #define MPS_INF_SKIP(a, v) ((a).skip ? (v) : R(INFINITY))
+
+// a near flag (near_wall, near_m) of the bucket of walk context c; a null table is "near"
+template <class R, class RN>
+__device__ __forceinline__ bool near_flag(const int8_t* f, const SceneDev<R, RN>& sc,
+                                          const RowCtx<R>& c) {
+    return !f || __ldg(f + sc.cbase + c.iz * sc.nbxy + c.iy * sc.nbx + c.ix) != 0;
+}
 
 // Phase 1 of a neighbour pass: the fluid neighbours j != s with d2 <= thr, in visiting
 // order, into the slot's list. Returns the neighbour count (may exceed nbK).
@@ -869,8 +881,9 @@ __device__ __forceinline__ void pass_a_finish(const PassArgs<R, RN>& a, const Sc
                                               const RowCtx<R>& c, R sx, R sy, R sz, int cf) {
     int cm = 0;
     if (TAPE) a.nbcnt[s] = cf;  // the recorded list (complete while cf <= nbK)
-    visc_sum_mirrors(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.m, MPS_INF_SKIP(a, sc.skip_r), sx, sy, sz,
-                     cm);
+    if (near_flag(a.near_m, sc, c))
+        visc_sum_mirrors(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.m, MPS_INF_SKIP(a, sc.skip_r), sx,
+                         sy, sz, cm);
     R ax = fmaR(sc.kn, sx, sc.g[0]), ay = fmaR(sc.kn, sy, sc.g[1]), az = fmaR(sc.kn, sz, sc.g[2]);
     R ux = fmaR(ax, sc.dt, v.x), uy = fmaR(ay, sc.dt, v.y), uz = fmaR(az, sc.dt, v.z);
     R x = fmaR(ux, sc.dt, p.x), y = fmaR(uy, sc.dt, p.y), z = fmaR(uz, sc.dt, p.z);
@@ -1098,7 +1111,9 @@ __global__ void __launch_bounds__(128, pass_b_blocks<R>(ALT))
         add(j, ldg4(pos + j));
     }
     col_dens_walls_mirrors<R, RN, true, true>(sc, c, p.x, p.y, p.z, v.x, v.y, v.z, a.wl, a.m,
-                                              a.skip != 0, wx, wy, wz, ni, cnt5);
+                                              a.skip != 0, wx, wy, wz, ni, cnt5,
+                                              near_flag(a.near_wall, sc, c),
+                                              near_flag(a.near_m, sc, c));
     pass_b_store<R, RN, DIAG>(a, sc, s, pid, wx, wy, wz, ni, cnt5);
 }
 
@@ -1238,7 +1253,8 @@ __global__ void __launch_bounds__(128, pass_c_blocks<R>(ALT, CORR))
         const int j = nb[k * st];
         gr(ldg4(pos + j), __ldg(prs + j));
     }
-    grad_sum_mirrors(sc, c, pid - sc.pbase, p.x, p.y, p.z, pmin, a.m, a.skip != 0, g, cm);
+    if (near_flag(a.near_m, sc, c))
+        grad_sum_mirrors(sc, c, pid - sc.pbase, p.x, p.y, p.z, pmin, a.m, a.skip != 0, g, cm);
     pass_c_finish<R, RN, DIAG, TAPE>(a, sc, s, pid, p, pi, g, cf, cm);
 }
 

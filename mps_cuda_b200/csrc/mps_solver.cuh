@@ -377,6 +377,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     int* nb;
     int* nbcnt;
     int8_t* near_wall;
+    int8_t *near_m1, *near_m2;  // near flags of the mirror tables M1 / M2 (k_near_wall on mcs)
     static constexpr int kListCap = 160;  // about 125 neighbours lie inside r at rest density
     int nbK = kListCap;                    // list capacity in use (MPS_OPT_LIST_CAPACITY)
     std::vector<int> fluid_ids, wall_ids;
@@ -654,12 +655,16 @@ template <class R, class RN> class Solver final : public SolverBase {
         d_integ = ar.template get<double>(6 * size_t(nscene));
         nb = ar.template get<int>(size_t(kListCap) * ((F + 31) / 32 * 32));  // list_at tiles
         near_wall = ar.template get<int8_t>(L());
+        near_m1 = ar.template get<int8_t>(L());
+        near_m2 = ar.template get<int8_t>(L());
         nbcnt = ar.template get<int>(F);
         CK(cudaMemsetAsync(S.acc, 0, sizeof(V4<R>) * F, stream));
         CK(cudaMemsetAsync(S2.acc, 0, sizeof(V4<R>) * F, stream));
         CK(cudaMemsetAsync(M1.slot, 0, sizeof(int) * cap, stream));
         CK(cudaMemsetAsync(mcs1, 0, sizeof(int) * (L() + 1), stream));
         CK(cudaMemsetAsync(mcs2, 0, sizeof(int) * (L() + 1), stream));
+        CK(cudaMemsetAsync(near_m1, 1, L(), stream));  // walk everywhere until a mirror build
+        CK(cudaMemsetAsync(near_m2, 1, L(), stream));
     }
 
     // ---- bucket build ------------------------------------------------------------------
@@ -730,6 +735,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         MirrorKeySrc<R, RN> ks{d_sc, nscene, dead(), U.pos, U.slot};
         MirrorGather<R> g{U.pos, U.slot, dst.pos, dst.slot};
         bin(ks, g, &cnt->mirror_raw, cap, dcs, L());
+        if (dcs == mcs1 || dcs == mcs2) near_flags(dcs, dcs == mcs1 ? near_m1 : near_m2);
     }
 
     WallView<R> wall_view() const { return WallView<R>{wcs, w_pos, w_nrm, w_vel, w_se, w_typ}; }
@@ -750,6 +756,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         a.cnt = cnt; a.diag = diag; a.ndens = ndens;
         a.nb = nb; a.nbcnt = nbcnt; a.nbK = nbK;
         a.near_wall = near_wall;
+        a.near_m = mcs == mcs1 ? near_m1 : (mcs == mcs2 ? near_m2 : nullptr);
         a.tape_pre = nullptr;
         return a;
     }
@@ -775,9 +782,10 @@ template <class R, class RN> class Solver final : public SolverBase {
         near_wall_flags();
     }
 
-    void near_wall_flags() {
+    void near_wall_flags() { near_flags(wcs, near_wall); }
+    void near_flags(const int* table_cs, int8_t* out) {
         dim3 g(std::max(1, std::min(blocks(C, 256), 148 * 4)), nscene);
-        k_near_wall<R, RN><<<g, 256, 0, stream>>>(d_sc, nscene, wcs, near_wall);
+        k_near_wall<R, RN><<<g, 256, 0, stream>>>(d_sc, nscene, table_cs, out);
         KL();
     }
 
@@ -1542,6 +1550,7 @@ template <class R, class RN> class Solver final : public SolverBase {
                               int* nbc, V4<R>* pre) {
         PassArgs<R, RN> a = args(M1, mcs1);
         a.m = MirrorView<R>{mcs, mpos, mslot};
+        a.near_m = nullptr;  // the recorded mirror tables carry no near flags
         a.nb = nbl;
         a.nbcnt = nbc;
         a.tape_pre = pre;

@@ -130,39 +130,6 @@ __global__ void k_bin_key(Src src, const int* n_ptr, int n_fixed, int* __restric
 }
 
 
-// k_bin_key for the fluid: also counts each fine cell's items at its row-major index
-template <class R, class RN>
-__global__ void k_bin_key_fluid(FluidKeySrc<R, RN> src, int n, int* __restrict__ key,
-                                int* __restrict__ rnk, int* __restrict__ count,
-                                int* __restrict__ count_r, DevCounters* cnt) {
-    const int lane = threadIdx.x & 31;
-    const int stride = gridDim.x * blockDim.x;
-    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
-        int t = base + lane;
-        bool act = t < n;
-        int c = act ? src.key(t, cnt) : -1;
-        unsigned peers = __match_any_sync(0xffffffffu, c);
-        int leader = __ffs(peers) - 1;
-        int below = __popc(peers & ((1u << lane) - 1));
-        int b = 0;
-        if (act && lane == leader) {
-            b = atomicAdd(&count[c], __popc(peers));
-            int cr = c;
-            if (c != src.dead) {
-                const SceneDev<R, RN>& s =
-                    src.sc[src.nscene > 1 ? scene_of(src.sc, src.nscene, src.pid[t]) : 0];
-                cr = fine_rowmajor(s, c);
-            }
-            atomicAdd(&count_r[cr], __popc(peers));
-        }
-        b = __shfl_sync(0xffffffffu, b, leader);
-        if (act) {
-            key[t] = c;
-            rnk[t] = b + below;
-        }
-    }
-}
-
 template <class Src>
 __global__ void k_bin_seg(Src src, const int* n_ptr, int n_fixed, const int* __restrict__ key,
                           const int* __restrict__ rnk, const int* __restrict__ cs,
@@ -350,9 +317,9 @@ static __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const int* _
     if (base <= L - 1 && L - 1 < base + kScanPer) out[L] = excl;  // thread holding the last item
 }
 
-// Scan of the fluid's fine-cell counts (fine_scan below): 16 counts per thread through int4
+// Scan of a bucket build's counts (k_fine_scan below): 16 counts per thread through int4
 // loads, and the counts cleared as they are read, so that the next bucket build starts from
-// zeros without a memset (the fine tables are 27 times the bucket count).
+// zeros without a memset.
 
 __device__ __forceinline__ void load16(const int* __restrict__ in, int base, int L, int v[16]) {
     if (base + 16 <= L) {
@@ -368,9 +335,8 @@ __device__ __forceinline__ void load16(const int* __restrict__ in, int base, int
     }
 }
 
-// Count tables of a bucket build with their per-tile totals (from the key kernel, or from
-// k_fine_tile_sums): the fluid build's two fine-cell tables (k = 0: bucket-major, 1:
-// row-major), or one bucket table (gridDim.y = 1), count[k] scanned into out[k].
+// Count tables of a bucket build with their per-tile totals (from the key kernel): the wall
+// and mirror builds' bucket tables (gridDim.y = 1), count[k] scanned into out[k].
 struct FineScan {
     int* count[2];
     int* part[2];
@@ -378,18 +344,6 @@ struct FineScan {
     int L, ntile;
     int* ticket;  // blocks finished; zero between launches
 };
-
-// part[k][b] = sum of count[k] over tile b (kScan16Tile entries), for k = blockIdx.y
-static __global__ void __launch_bounds__(kScan16Threads) k_fine_tile_sums(FineScan f) {
-    __shared__ int sh[32];
-    int v[16];
-    load16(f.count[blockIdx.y], blockIdx.x * kScan16Tile + threadIdx.x * kScan16Per, f.L, v);
-    int s = 0;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) s += v[k];
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0) f.part[blockIdx.y][blockIdx.x] = s;
-}
 
 // Exclusive scan of count[k][0..L) into out[k][0..L], out[k][L] = total, for k = blockIdx.y.
 // The counts are left zero; the last block to finish also zeroes the tile totals for the
@@ -462,6 +416,261 @@ static __global__ void __launch_bounds__(kScan16Threads) k_fine_scan(FineScan f)
         for (int k = threadIdx.x; k < f.ntile; k += blockDim.x)
             for (int y = 0; y < int(gridDim.y); ++y) f.part[y][k] = 0;
         if (threadIdx.x == 0) *f.ticket = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// start tables of the fluid build from one count table, by bucket rows
+// ---------------------------------------------------------------------------------------
+// The fluid's fine cells are counted once, bucket-major (27 per bucket, 9 sz + 3 sy + sx).
+// A bucket row (one scene's buckets at iz, iy, every ix) holds 27 nbx of them: nine fine
+// rows (3 iz + sz, 3 iy + sy) of 3 nbx cells each, interleaved bucket by bucket. Both start
+// tables follow from per-row totals: the bucket-major one (cs) from each bucket row's total,
+// the row-major one (csr, the order of posf) from each fine row's total. One block per
+// bucket row totals its counts (k_fine_rows_sum), one block per table scans the totals
+// (k_fine_rows_scan), and one block per bucket row writes both tables and clears its counts
+// (k_fine_rows_write): the counts are read twice and cleared once, with no second count
+// table and no second count atomic per item. (Taking the row totals in the key kernel
+// instead, with one atomic per group of a warp's items in a row, was measured slower: the
+// write pass then met the counts cold in DRAM.)
+struct FineRows {
+    int* count;          // bucket-major fine-cell counts (cleared by k_fine_rows_write)
+    int* brtot;          // per bucket row (scene, iz, iy): its total, then its start
+    int* frtot;          // per fine row (scene, fz, fy): its total, then its start
+    int* cs;             // bucket-major starts, [0, dead + 1]
+    int* csr;            // row-major starts, [0, dead + 1]
+    const int* rowscan;  // per scene: bucket rows before it (nscene + 1 entries)
+    int nscene, nrows;   // bucket rows of all scenes
+    int dead;            // the unlisted items' cell, after every scene's cells
+};
+
+template <class R, class RN>
+__device__ __forceinline__ const SceneDev<R, RN>& bucket_row(const FineRows& f,
+                                                             const SceneDev<R, RN>* scs, int r,
+                                                             int& s, int& iz, int& iy) {
+    int lo = 0, hi = f.nscene;  // rowscan[lo] <= r < rowscan[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(f.rowscan + mid) <= r) lo = mid; else hi = mid;
+    }
+    s = lo;
+    const SceneDev<R, RN>& sc = scs[s];
+    const int lr = r - __ldg(f.rowscan + s);
+    iz = lr / sc.nby;
+    iy = lr - iz * sc.nby;
+    return sc;
+}
+
+// fine row index (scene base + fz 3 nby + fy) of fine row q = 3 sz + sy of bucket row (iz, iy)
+template <class R, class RN>
+__device__ __forceinline__ int fine_row_of(const FineRows& f, const SceneDev<R, RN>& sc, int s,
+                                           int iz, int iy, int q) {
+    return 9 * __ldg(f.rowscan + s) + (3 * iz + q / 3) * (3 * sc.nby) + 3 * iy + q % 3;
+}
+
+// inclusive warp scan of v (all lanes)
+__device__ __forceinline__ int warp_incl(int v) {
+    const int lane = threadIdx.x & 31;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+    }
+    return v;
+}
+
+constexpr int kRowThreads = 256;
+
+// exclusive block scan of the N values of every thread; tot receives the block totals.
+// sh: N * (kRowThreads / 32) ints of shared memory
+template <int N>
+__device__ __forceinline__ void block_exscan(int (&v)[N], int (&tot)[N], int* sh) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int inc[N];
+#pragma unroll
+    for (int q = 0; q < N; ++q) inc[q] = warp_incl(v[q]);
+    __syncthreads();
+    if (lane == 31)
+#pragma unroll
+        for (int q = 0; q < N; ++q) sh[q * 32 + w] = inc[q];
+    __syncthreads();
+    if (w == 0)
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+            const int x = lane < nw ? sh[q * 32 + lane] : 0;
+            sh[q * 32 + lane] = warp_incl(x);  // inclusive over warps
+        }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+        const int before = w > 0 ? sh[q * 32 + w - 1] : 0;
+        tot[q] = sh[q * 32 + nw - 1];
+        v[q] = before + inc[q] - v[q];
+    }
+    __syncthreads();
+}
+
+// A chunk of kRowThreads buckets of a bucket row moves between global and shared memory with
+// coalesced loads and stores; each thread then works on its own bucket's 27 counts there
+// (stride 27, odd: no bank conflicts).
+constexpr int kRowChunk = 27 * kRowThreads;
+
+template <class R, class RN>
+__global__ void __launch_bounds__(kRowThreads) k_fine_rows_sum(FineRows f,
+                                                                const SceneDev<R, RN>* scs) {
+    __shared__ int sh[9 * 32];
+    __shared__ int buf[kRowChunk];
+    int s, iz, iy;
+    const SceneDev<R, RN>& sc = bucket_row(f, scs, blockIdx.x, s, iz, iy);
+    const int* __restrict__ cnt = f.count + sc.fbase + 27 * (iz * sc.nbxy + iy * sc.nbx);
+    int t9[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) t9[q] = 0;
+    for (int b0 = 0; b0 < sc.nbx; b0 += kRowThreads) {
+        const int n = 27 * min(kRowThreads, sc.nbx - b0);
+        __syncthreads();
+        // unrolled with a fixed trip count, so that a thread's 27 loads are in flight together
+#pragma unroll
+        for (int j = 0; j < 27; ++j) {
+            const int i = threadIdx.x + j * kRowThreads;
+            if (i < n) buf[i] = __ldg(cnt + 27 * b0 + i);
+        }
+        __syncthreads();
+        if (27 * threadIdx.x < n)
+#pragma unroll
+            for (int k = 0; k < 27; ++k) t9[k / 3] += buf[27 * threadIdx.x + k];
+    }
+    int tot[9];
+    block_exscan<9>(t9, tot, sh);
+    if (threadIdx.x == 0) {
+        int all = 0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            f.frtot[fine_row_of(f, sc, s, iz, iy, q)] = tot[q];
+            all += tot[q];
+        }
+        f.brtot[blockIdx.x] = all;
+    }
+}
+
+// exclusive scan in place of brtot (block 0, nrows entries) and frtot (block 1, 9 nrows);
+// block 0 also closes both tables with the unlisted cell and clears its count. Each warp
+// scans one contiguous segment 32 entries at a time (coalesced), after one pass that totals
+// the segments.
+static __global__ void __launch_bounds__(1024) k_fine_rows_scan(FineRows f) {
+    __shared__ int sh[32];
+    int* a = blockIdx.x == 0 ? f.brtot : f.frtot;
+    const int n = blockIdx.x == 0 ? f.nrows : 9 * f.nrows;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int seg = (n + nw - 1) / nw;
+    const int lo = min(n, w * seg), hi = min(n, lo + seg);
+    int sum = 0;
+    for (int k = lo + lane; k < hi; k += 32) sum += a[k];
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) sh[w] = sum;
+    __syncthreads();
+    if (w == 0) {
+        const int x = lane < nw ? sh[lane] : 0;
+        const int inc = warp_incl(x);
+        __syncwarp();
+        sh[lane] = inc - x;  // exclusive start of each warp's segment
+        if (blockIdx.x == 0 && lane == 31) {
+            const int total = inc;  // every listed item
+            const int nd = f.count[f.dead];
+            f.cs[f.dead] = total;
+            f.cs[f.dead + 1] = total + nd;
+            f.csr[f.dead] = total;
+            f.csr[f.dead + 1] = total + nd;
+            f.count[f.dead] = 0;
+        }
+    }
+    __syncthreads();
+    int run = sh[w];
+    for (int k0 = lo; k0 < hi; k0 += 32) {
+        const int k = k0 + lane;
+        const int x = k < hi ? a[k] : 0;
+        const int inc = warp_incl(x);
+        if (k < hi) a[k] = run + inc - x;
+        run += __shfl_sync(0xffffffffu, inc, 31);
+    }
+}
+
+template <class R, class RN>
+__global__ void __launch_bounds__(kRowThreads) k_fine_rows_write(FineRows f,
+                                                                  const SceneDev<R, RN>* scs) {
+    __shared__ int sh[10 * 32];
+    __shared__ int carry[10];  // bucket-major, then the nine fine rows
+    __shared__ int buf[kRowChunk];
+    int s, iz, iy;
+    const SceneDev<R, RN>& sc = bucket_row(f, scs, blockIdx.x, s, iz, iy);
+    const int cb = sc.fbase + 27 * (iz * sc.nbxy + iy * sc.nbx);
+    int* __restrict__ cnt = f.count + cb;
+    if (threadIdx.x < 10)
+        carry[threadIdx.x] = threadIdx.x == 0
+                                 ? __ldg(f.brtot + blockIdx.x)
+                                 : __ldg(f.frtot + fine_row_of(f, sc, s, iz, iy, threadIdx.x - 1));
+    const int nfx = 3 * sc.nbx, nfxy = 9 * sc.nbxy;
+    for (int b0 = 0; b0 < sc.nbx; b0 += kRowThreads) {
+        const int nb = min(kRowThreads, sc.nbx - b0), n = 27 * nb;
+        const bool act = int(threadIdx.x) < nb;
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 27; ++j) {
+            const int i = threadIdx.x + j * kRowThreads;
+            if (i < n) buf[i] = cnt[27 * b0 + i];
+        }
+        __syncthreads();
+        int c[27];
+#pragma unroll
+        for (int k = 0; k < 27; ++k) c[k] = act ? buf[27 * threadIdx.x + k] : 0;
+        int v[10], tot[10];
+        v[0] = 0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            v[q + 1] = c[3 * q] + c[3 * q + 1] + c[3 * q + 2];
+            v[0] += v[q + 1];
+        }
+        block_exscan<10>(v, tot, sh);  // also orders the reads of buf before the writes below
+        // bucket-major starts, through buf
+        if (act) {
+            int run = carry[0] + v[0];
+#pragma unroll
+            for (int k = 0; k < 27; ++k) {
+                buf[27 * threadIdx.x + k] = run;
+                run += c[k];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < 27; ++j) {
+            const int i = threadIdx.x + j * kRowThreads;
+            if (i < n) {
+                f.cs[cb + 27 * b0 + i] = buf[i];
+                cnt[27 * b0 + i] = 0;  // the counts back to zero for the next build
+            }
+        }
+        // row-major starts: fine row q's 3 nb cells of this chunk are contiguous in csr
+        __syncthreads();
+        if (act)
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                int r = carry[q + 1] + v[q + 1];
+#pragma unroll
+                for (int x = 0; x < 3; ++x) {
+                    buf[q * 3 * kRowThreads + 3 * threadIdx.x + x] = r;
+                    r += c[3 * q + x];
+                }
+            }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            int* o = f.csr + sc.fbase + (3 * iz + q / 3) * nfxy + (3 * iy + q % 3) * nfx + 3 * b0;
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const int i = threadIdx.x + j * kRowThreads;
+                if (i < 3 * nb) o[i] = buf[q * 3 * kRowThreads + i];
+            }
+        }
+        if (threadIdx.x < 10) carry[threadIdx.x] += tot[threadIdx.x];
     }
 }
 

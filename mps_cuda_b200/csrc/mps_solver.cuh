@@ -361,8 +361,11 @@ template <class R, class RN> class Solver final : public SolverBase {
     int* cs;
     // fluid positions in row-major fine-cell order (slot in w) and that order's cell starts
     V4<R>* posf;
-    int *csr, *count_f, *count_r;
-    int *part_f, *part_r;  // per scan tile totals of count_f / count_r (k_fine_tile_sums)
+    int *csr, *count_f;
+    // the fluid build's start tables by bucket rows (k_fine_rows_*): per bucket row and per
+    // fine row totals, then starts; per scene the bucket rows before it
+    int *row_tot, *frow_tot, *row_scan;
+    int nrows = 0;
     bool posf_stale = false;  // particles moved in place since the copy was made
     // bucket-build scratch
     int *key, *rnk, *seg, *count, *part;
@@ -613,16 +616,20 @@ template <class R, class RN> class Solver final : public SolverBase {
         wcs = ar.template get<int>(L() + 1);
         cs = ar.template get<int>(size_t(LF()) + 1);
         csr = ar.template get<int>(size_t(LF()) + 1);
-        // the fluid's own count tables: its scans leave them zero for the next build
+        // the fluid's own count table: the start-table pass leaves it zero for the next build
         count_f = ar.template get<int>(size_t(LF()));
-        count_r = ar.template get<int>(size_t(LF()));
         CK(cudaMemsetAsync(count_f, 0, sizeof(int) * size_t(LF()), stream));
-        CK(cudaMemsetAsync(count_r, 0, sizeof(int) * size_t(LF()), stream));
-        const size_t ntile = (size_t(LF()) + kScan16Tile - 1) / kScan16Tile;
-        part_f = ar.template get<int>(ntile);
-        part_r = ar.template get<int>(ntile);
-        CK(cudaMemsetAsync(part_f, 0, sizeof(int) * ntile, stream));
-        CK(cudaMemsetAsync(part_r, 0, sizeof(int) * ntile, stream));
+        {
+            std::vector<int> rs(nscene + 1, 0);
+            for (int s = 0; s < nscene; ++s) rs[s + 1] = rs[s] + hsc[s].nby * hsc[s].nbz;
+            nrows = rs[nscene];
+            row_scan = ar.template get<int>(rs.size());
+            row_tot = ar.template get<int>(size_t(nrows));
+            frow_tot = ar.template get<int>(9 * size_t(nrows));
+            CK(cudaMemcpyAsync(row_scan, rs.data(), sizeof(int) * rs.size(), cudaMemcpyHostToDevice,
+                               stream));
+            CK(cudaStreamSynchronize(stream));  // rs leaves scope
+        }
         posf = ar.template get<V4<R>>(F);
         for (MirrorBuf<R>* b : {&U, &M1, &M2}) {
             b->pos = ar.template get<V4<R>>(cap);
@@ -701,17 +708,18 @@ template <class R, class RN> class Solver final : public SolverBase {
         FluidGatherF<R, RN> g{{pos, vel, acc, prs, pav, pid, typ, S2.pos, S2.vel, S2.acc, S2.prs,
                                S2.pav, S2.pid, S2.typ},
                               d_sc, nscene, key, cs, csr, posf};
-        const int ncell = LF();
         const int grid = std::min(blocks(std::max(nF, 1), 256), 148 * 32);
         if (nF > 0) {
-            k_bin_key_fluid<R, RN><<<grid, 256, 0, stream>>>(ks, nF, key, rnk, count_f, count_r, cnt);
+            k_bin_key<FluidKeySrc<R, RN>><<<grid, 256, 0, stream>>>(ks, nullptr, nF, key, rnk,
+                                                                    count_f, nullptr, cnt);
             KL();
         }
-        const int nb = (ncell + kScan16Tile - 1) / kScan16Tile;
-        FineScan fs{{count_f, count_r}, {part_f, part_r}, {cs, csr}, ncell, nb, &cnt->scan_ticket};
-        k_fine_tile_sums<<<dim3(nb, 2), kScan16Threads, 0, stream>>>(fs);
+        FineRows fr{count_f, row_tot, frow_tot, cs, csr, row_scan, nscene, nrows, deadF()};
+        k_fine_rows_sum<R, RN><<<nrows, kRowThreads, 0, stream>>>(fr, d_sc);
         KL();
-        k_fine_scan<<<dim3(nb, 2), kScan16Threads, 0, stream>>>(fs);
+        k_fine_rows_scan<<<2, 1024, 0, stream>>>(fr);
+        KL();
+        k_fine_rows_write<R, RN><<<nrows, kRowThreads, 0, stream>>>(fr, d_sc);
         KL();
         if (nF > 0) {
             k_bin_seg<FluidKeySrc<R, RN>><<<grid, 256, 0, stream>>>(ks, nullptr, nF, key, rnk, cs, seg);

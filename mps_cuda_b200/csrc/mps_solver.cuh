@@ -985,7 +985,8 @@ template <class R, class RN> class Solver final : public SolverBase {
     //                    for the walk through L1, and the staged walk at 128 threads;
     //   passes B, C and mirror generation: 128, 96, 64 or 32 threads per block;
     //   then passes B, C and A at their alternate register bound, with the chosen shapes.
-    // All groups are timed in the same trial steps (they are separate kernels). The state is
+    // All groups are timed in the same trial steps (they are separate kernels), and every
+    // round starts from the handle's state (restored from a snapshot). The state is
     // restored afterwards, and the choice is kept for later handles of the same precision
     // and size class in this process (tuned_cache).
     void autotune(int trial, int32_t* chosen) override {
@@ -1015,6 +1016,9 @@ template <class R, class RN> class Solver final : public SolverBase {
             const bool new_b = i < 4;
             if (new_b)
                 for (int g : groups_b) blk[g] = cand_b[i];
+            // every candidate runs the same steps from the snapshot (a dam break's steps
+            // grow slower as it evolves, which would favour the candidates tried first)
+            load_fluid(true);
             step(trial);
             auto read = [&](int g, double& ms_per) {
                 double ms = 0;
@@ -1043,6 +1047,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         batch_a = best_batch;
         // the alternate register bounds of passes B, C and A, at the chosen shapes
         reg_bound = 7;
+        load_fluid(true);
         step(trial);
         int regb = 0;
         {

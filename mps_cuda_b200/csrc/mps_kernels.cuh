@@ -478,10 +478,8 @@ __device__ __forceinline__ int warp_incl(int v) {
     return v;
 }
 
-constexpr int kRowThreads = 256;
-
 // exclusive block scan of the N values of every thread; tot receives the block totals.
-// sh: N * (kRowThreads / 32) ints of shared memory
+// sh: N * 32 ints of shared memory
 template <int N>
 __device__ __forceinline__ void block_exscan(int (&v)[N], int (&tot)[N], int* sh) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -509,29 +507,29 @@ __device__ __forceinline__ void block_exscan(int (&v)[N], int (&tot)[N], int* sh
     __syncthreads();
 }
 
-// A chunk of kRowThreads buckets of a bucket row moves between global and shared memory with
-// coalesced loads and stores; each thread then works on its own bucket's 27 counts there
-// (stride 27, odd: no bank conflicts).
-constexpr int kRowChunk = 27 * kRowThreads;
+// A chunk of T buckets of a bucket row (T threads per block: 64, 128 or 256, the handle's
+// longest bucket row rounded up, so that short rows do not leave most threads idle) moves
+// between global and shared memory with coalesced loads and stores; each thread then works on
+// its own bucket's 27 counts there (stride 27, odd: no bank conflicts).
 
-template <class R, class RN>
-__global__ void __launch_bounds__(kRowThreads) k_fine_rows_sum(FineRows f,
+template <class R, class RN, int T>
+__global__ void __launch_bounds__(T) k_fine_rows_sum(FineRows f,
                                                                 const SceneDev<R, RN>* scs) {
     __shared__ int sh[9 * 32];
-    __shared__ int buf[kRowChunk];
+    __shared__ int buf[27 * T];
     int s, iz, iy;
     const SceneDev<R, RN>& sc = bucket_row(f, scs, blockIdx.x, s, iz, iy);
     const int* __restrict__ cnt = f.count + sc.fbase + 27 * (iz * sc.nbxy + iy * sc.nbx);
     int t9[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) t9[q] = 0;
-    for (int b0 = 0; b0 < sc.nbx; b0 += kRowThreads) {
-        const int n = 27 * min(kRowThreads, sc.nbx - b0);
+    for (int b0 = 0; b0 < sc.nbx; b0 += T) {
+        const int n = 27 * min(T, sc.nbx - b0);
         __syncthreads();
         // unrolled with a fixed trip count, so that a thread's 27 loads are in flight together
 #pragma unroll
         for (int j = 0; j < 27; ++j) {
-            const int i = threadIdx.x + j * kRowThreads;
+            const int i = threadIdx.x + j * T;
             if (i < n) buf[i] = __ldg(cnt + 27 * b0 + i);
         }
         __syncthreads();
@@ -564,6 +562,7 @@ static __global__ void __launch_bounds__(1024) k_fine_rows_scan(FineRows f) {
     const int seg = (n + nw - 1) / nw;
     const int lo = min(n, w * seg), hi = min(n, lo + seg);
     int sum = 0;
+#pragma unroll 4
     for (int k = lo + lane; k < hi; k += 32) sum += a[k];
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     if (lane == 0) sh[w] = sum;
@@ -585,21 +584,29 @@ static __global__ void __launch_bounds__(1024) k_fine_rows_scan(FineRows f) {
     }
     __syncthreads();
     int run = sh[w];
-    for (int k0 = lo; k0 < hi; k0 += 32) {
-        const int k = k0 + lane;
-        const int x = k < hi ? a[k] : 0;
-        const int inc = warp_incl(x);
-        if (k < hi) a[k] = run + inc - x;
-        run += __shfl_sync(0xffffffffu, inc, 31);
+    for (int k0 = lo; k0 < hi; k0 += 128) {  // four loads in flight per lane
+        int x[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int k = k0 + 32 * j + lane;
+            x[j] = k < hi ? a[k] : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int k = k0 + 32 * j + lane;
+            const int inc = warp_incl(x[j]);
+            if (k < hi) a[k] = run + inc - x[j];
+            run += __shfl_sync(0xffffffffu, inc, 31);
+        }
     }
 }
 
-template <class R, class RN>
-__global__ void __launch_bounds__(kRowThreads) k_fine_rows_write(FineRows f,
+template <class R, class RN, int T>
+__global__ void __launch_bounds__(T) k_fine_rows_write(FineRows f,
                                                                   const SceneDev<R, RN>* scs) {
     __shared__ int sh[10 * 32];
     __shared__ int carry[10];  // bucket-major, then the nine fine rows
-    __shared__ int buf[kRowChunk];
+    __shared__ int buf[27 * T];
     int s, iz, iy;
     const SceneDev<R, RN>& sc = bucket_row(f, scs, blockIdx.x, s, iz, iy);
     const int cb = sc.fbase + 27 * (iz * sc.nbxy + iy * sc.nbx);
@@ -609,13 +616,13 @@ __global__ void __launch_bounds__(kRowThreads) k_fine_rows_write(FineRows f,
                                  ? __ldg(f.brtot + blockIdx.x)
                                  : __ldg(f.frtot + fine_row_of(f, sc, s, iz, iy, threadIdx.x - 1));
     const int nfx = 3 * sc.nbx, nfxy = 9 * sc.nbxy;
-    for (int b0 = 0; b0 < sc.nbx; b0 += kRowThreads) {
-        const int nb = min(kRowThreads, sc.nbx - b0), n = 27 * nb;
+    for (int b0 = 0; b0 < sc.nbx; b0 += T) {
+        const int nb = min(T, sc.nbx - b0), n = 27 * nb;
         const bool act = int(threadIdx.x) < nb;
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < 27; ++j) {
-            const int i = threadIdx.x + j * kRowThreads;
+            const int i = threadIdx.x + j * T;
             if (i < n) buf[i] = cnt[27 * b0 + i];
         }
         __syncthreads();
@@ -642,7 +649,7 @@ __global__ void __launch_bounds__(kRowThreads) k_fine_rows_write(FineRows f,
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < 27; ++j) {
-            const int i = threadIdx.x + j * kRowThreads;
+            const int i = threadIdx.x + j * T;
             if (i < n) {
                 f.cs[cb + 27 * b0 + i] = buf[i];
                 cnt[27 * b0 + i] = 0;  // the counts back to zero for the next build
@@ -656,7 +663,7 @@ __global__ void __launch_bounds__(kRowThreads) k_fine_rows_write(FineRows f,
                 int r = carry[q + 1] + v[q + 1];
 #pragma unroll
                 for (int x = 0; x < 3; ++x) {
-                    buf[q * 3 * kRowThreads + 3 * threadIdx.x + x] = r;
+                    buf[q * 3 * T + 3 * threadIdx.x + x] = r;
                     r += c[3 * q + x];
                 }
             }
@@ -666,8 +673,8 @@ __global__ void __launch_bounds__(kRowThreads) k_fine_rows_write(FineRows f,
             int* o = f.csr + sc.fbase + (3 * iz + q / 3) * nfxy + (3 * iy + q % 3) * nfx + 3 * b0;
 #pragma unroll
             for (int j = 0; j < 3; ++j) {
-                const int i = threadIdx.x + j * kRowThreads;
-                if (i < 3 * nb) o[i] = buf[q * 3 * kRowThreads + i];
+                const int i = threadIdx.x + j * T;
+                if (i < 3 * nb) o[i] = buf[q * 3 * T + i];
             }
         }
         if (threadIdx.x < 10) carry[threadIdx.x] += tot[threadIdx.x];

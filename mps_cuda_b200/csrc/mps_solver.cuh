@@ -366,6 +366,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     // fine row totals, then starts; per scene the bucket rows before it
     int *row_tot, *frow_tot, *row_scan;
     int nrows = 0;
+    int row_threads = 256;  // threads per bucket row block: the longest row rounded up
     bool posf_stale = false;  // particles moved in place since the copy was made
     // bucket-build scratch
     int *key, *rnk, *seg, *count, *part;
@@ -623,6 +624,9 @@ template <class R, class RN> class Solver final : public SolverBase {
             std::vector<int> rs(nscene + 1, 0);
             for (int s = 0; s < nscene; ++s) rs[s + 1] = rs[s] + hsc[s].nby * hsc[s].nbz;
             nrows = rs[nscene];
+            int nbx_max = 0;
+            for (int s = 0; s < nscene; ++s) nbx_max = std::max(nbx_max, hsc[s].nbx);
+            row_threads = nbx_max <= 64 ? 64 : (nbx_max <= 128 ? 128 : 256);
             row_scan = ar.template get<int>(rs.size());
             row_tot = ar.template get<int>(size_t(nrows));
             frow_tot = ar.template get<int>(9 * size_t(nrows));
@@ -715,12 +719,9 @@ template <class R, class RN> class Solver final : public SolverBase {
             KL();
         }
         FineRows fr{count_f, row_tot, frow_tot, cs, csr, row_scan, nscene, nrows, deadF()};
-        k_fine_rows_sum<R, RN><<<nrows, kRowThreads, 0, stream>>>(fr, d_sc);
-        KL();
-        k_fine_rows_scan<<<2, 1024, 0, stream>>>(fr);
-        KL();
-        k_fine_rows_write<R, RN><<<nrows, kRowThreads, 0, stream>>>(fr, d_sc);
-        KL();
+        if (row_threads == 64) fine_rows<64>(fr);
+        else if (row_threads == 128) fine_rows<128>(fr);
+        else fine_rows<256>(fr);
         if (nF > 0) {
             k_bin_seg<FluidKeySrc<R, RN>><<<grid, 256, 0, stream>>>(ks, nullptr, nF, key, rnk, cs, seg);
             KL();
@@ -731,6 +732,15 @@ template <class R, class RN> class Solver final : public SolverBase {
         std::swap(S, S2);
         ++swap_count;
         posf_stale = false;
+    }
+
+    template <int T> void fine_rows(const FineRows& fr) {
+        k_fine_rows_sum<R, RN, T><<<nrows, T, 0, stream>>>(fr, d_sc);
+        KL();
+        k_fine_rows_scan<<<2, 1024, 0, stream>>>(fr);
+        KL();
+        k_fine_rows_write<R, RN, T><<<nrows, T, 0, stream>>>(fr, d_sc);
+        KL();
     }
 
     void mkbkt(bool with_acc) {
@@ -792,7 +802,9 @@ template <class R, class RN> class Solver final : public SolverBase {
 
     void near_wall_flags() { near_flags(wcs, near_wall); }
     void near_flags(const int* table_cs, int8_t* out) {
-        dim3 g(std::max(1, std::min(blocks(C, 256), 148 * 4)), nscene);
+        int nb_max = 1;  // blocks along x cover the largest scene's buckets (y: the scenes)
+        for (int s = 0; s < nscene; ++s) nb_max = std::max(nb_max, hsc[s].nbxy * hsc[s].nbz);
+        dim3 g(std::max(1, std::min(blocks(nb_max, 256), 148 * 4)), nscene);
         k_near_wall<R, RN><<<g, 256, 0, stream>>>(d_sc, nscene, table_cs, out);
         KL();
     }

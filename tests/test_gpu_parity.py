@@ -318,3 +318,25 @@ def test_reads_between_steps_change_nothing(graph):
     _assert_same_state(g.state(), o.state(), "after")
     g.close()
     h.close()
+
+
+@pytest.mark.parametrize("prec", [F32, F64])
+def test_bucket_rows_longer_than_a_block_equal_the_oracle(prec):
+    """A tank 287 buckets long: the fluid build's start-table pass walks each bucket row in
+    several chunks of 256 buckets, carrying its running starts from chunk to chunk."""
+    from mps_cuda_b200 import SceneDesc, derive
+    desc = SceneDesc(0.004, (3.5, 0.06, 0.1), (30, 8, 10))
+    p = dambreak_params(desc, dt=4e-5, precision=prec)
+    assert derive(p).nbx > 256
+    sc = dambreak(desc)
+    d = _dt(prec)
+    args = (sc["typ"], sc["pos"].astype(d), sc["vel"].astype(d), sc["nrm"].astype(d))
+    g = MPS(p, *args)
+    o = Oracle(params_from(p), *args)
+    g.set_option(L.OPT_GRAPH, 1)
+    for chunk in (1, 3):
+        g.step(chunk)
+        o.step(chunk)
+        _assert_same_state(g.state(), o.state(), ("long tank", chunk))
+    _assert_same_mirrors(g.mirrors(2), o.mirrors())
+    g.close()

@@ -996,7 +996,8 @@ template <class R, class RN> class Solver final : public SolverBase {
     //   pass A (VscTrm): candidates in flight (2, 4, 8) and 128 or 64 threads per block
     //                    for the walk through L1, and the staged walk at 128 threads;
     //   passes B, C and mirror generation: 128, 96, 64 or 32 threads per block;
-    //   then passes B, C and A at their alternate register bound, with the chosen shapes.
+    //   then passes B, C and A at their alternate register bound, with the chosen shapes
+    //   (pass A with each candidate batch).
     // All groups are timed in the same trial steps (they are separate kernels), and every
     // round starts from the handle's state (restored from a snapshot). The state is
     // restored afterwards, and the choice is kept for later handles of the same precision
@@ -1057,26 +1058,38 @@ template <class R, class RN> class Solver final : public SolverBase {
         blk[MPS_K_PASS_A] = bestb[MPS_K_PASS_A];
         stage_mode = best_stage;
         batch_a = best_batch;
-        // the alternate register bounds of passes B, C and A, at the chosen shapes
-        reg_bound = 7;
-        load_fluid(true);
-        step(trial);
+        // the alternate register bounds of passes B, C and A, at the chosen shapes; pass A's
+        // bound and its candidate batch interact (fewer registers suit a smaller batch), so
+        // pass A tries the alternate bound with every batch
         int regb = 0;
-        {
+        const int chosen_batch = batch_a;
+        const int batches[3] = {chosen_batch, chosen_batch == 2 ? 4 : 2, chosen_batch == 8 ? 4 : 8};
+        for (int r = 0; r < 3; ++r) {
+            reg_bound = 7;
+            batch_a = batches[r];
+            load_fluid(true);
+            step(trial);
             double ms = 0;
             long long n = 0;
-            timing(MPS_K_PASS_B, &ms, &n, false);
-            if (n > 0 && ms / n < best[MPS_K_PASS_B]) regb |= 1;
-            ms = 0;
-            n = 0;
-            timing(MPS_K_PASS_C, &ms, &n, false);
-            if (n > 0 && ms / n < best[MPS_K_PASS_C]) regb |= 2;
-            ms = 0;
-            n = 0;
+            if (r == 0) {
+                timing(MPS_K_PASS_B, &ms, &n, false);
+                if (n > 0 && ms / n < best[MPS_K_PASS_B]) regb |= 1;
+                ms = 0;
+                n = 0;
+                timing(MPS_K_PASS_C, &ms, &n, false);
+                if (n > 0 && ms / n < best[MPS_K_PASS_C]) regb |= 2;
+                ms = 0;
+                n = 0;
+            }
             timing(MPS_K_PASS_A, &ms, &n, false);
-            if (stage_mode == MPS_STAGE_GLOBAL && n > 0 && ms / n < best[MPS_K_PASS_A]) regb |= 4;
+            if (stage_mode == MPS_STAGE_GLOBAL && n > 0 && ms / n < best[MPS_K_PASS_A]) {
+                best[MPS_K_PASS_A] = ms / n;
+                regb |= 4;
+                best_batch = batches[r];
+            }
             timing(0, nullptr, nullptr, true);
         }
+        batch_a = best_batch;
         reg_bound = regb;
         load_fluid(true);  // back to the snapshot: tuning leaves no trace in the results
         steps = steps0;

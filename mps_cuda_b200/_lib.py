@@ -34,6 +34,7 @@ OPT_DIAG, OPT_GRAPH, OPT_BLOCK, OPT_CELL_SKIP, OPT_TIMING, OPT_GRADIENT = 0, 1, 
 OPT_LIST_CAPACITY = 6
 OPT_STAGING, OPT_STAGE_CAPACITY, OPT_CANDIDATE_BATCH = 7, 8, 9
 OPT_REGISTER_BOUND = 10
+OPT_OVERLAP = 11
 STAGE_GLOBAL, STAGE_POSITIONS, STAGE_VELOCITIES = 0, 1, 2
 GRAD_STANDARD, GRAD_CORRECTED = 0, 1
 KERNEL_GROUPS = ["pass_a", "pass_b", "pass_c", "gen_cull", "bin_fluid", "bin_mirror"]

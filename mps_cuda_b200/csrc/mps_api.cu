@@ -208,6 +208,10 @@ int mps_set_option(mps_handle* h, int32_t opt, int32_t value) {
                 s.reg_bound = value;
                 s.invalidate_graph();
                 break;
+            case MPS_OPT_OVERLAP:
+                s.overlap_on = value != 0;
+                s.invalidate_graph();
+                break;
             case MPS_OPT_STAGE_CAPACITY:
                 if (value < 0 || value > (1 << 16))
                     throw ApiError(MPS_ERR_ARG, "stage capacity must lie in [0, 65536]");
@@ -240,6 +244,7 @@ int mps_get_option(mps_handle* h, int32_t opt, int32_t* value) {
             case MPS_OPT_STAGE_CAPACITY: *value = s.stage_cap; break;
             case MPS_OPT_CANDIDATE_BATCH: *value = s.batch_a; break;
             case MPS_OPT_REGISTER_BOUND: *value = s.reg_bound; break;
+            case MPS_OPT_OVERLAP: *value = s.overlap_on; break;
             default: throw ApiError(MPS_ERR_ARG, "unknown option");
         }
     });

@@ -274,6 +274,7 @@ struct SolverBase {
     int stage_cap = 0;                  // candidates staged per block (MPS_OPT_STAGE_CAPACITY)
     int batch_a = 4;                    // VscTrm's candidates in flight (MPS_OPT_CANDIDATE_BATCH)
     int reg_bound = 0;                  // passes B, C, A at their alternate register bound (bits 0-2)
+    bool overlap_on = true;             // the end of a step on two streams (MPS_OPT_OVERLAP)
     long long steps = 0;
     long long launches = 0;       // kernels launched (graph replays included)
     long long head_launches = 0;  // kernels of one captured step up to PrsGrdTrm
@@ -402,6 +403,26 @@ template <class R, class RN> class Solver final : public SolverBase {
     // slot order of S. It runs when the next step starts or when something reads the sorted
     // state, so a state replaced in between (mps_set_state) wastes no build.
     bool tail_pending = false;
+    // the second stream of a step's end (overlap_on), created at its first use, at the
+    // device's highest priority so that the bucket build's short scan launches get SMs while
+    // the mirror generation's blocks are pending; the fork and join events
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    void ensure_side() {
+        if (side) return;
+        int lo = 0, hi = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        CK(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, hi));
+    }
+    // launches issued in its scope go to stream `to`; the handle's stream is restored on exit
+    struct OnStream {
+        Solver* s;
+        cudaStream_t prev;
+        OnStream(Solver* s_, cudaStream_t to) : s(s_), prev(s_->stream) { s->stream = to; }
+        ~OnStream() { s->stream = prev; }
+    };
     // CUDA events bracketing kernel groups when timing_on
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
@@ -469,6 +490,12 @@ template <class R, class RN> class Solver final : public SolverBase {
             cudaEventDestroy(pe.second.second);
         }
         for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+        if (side) {
+            cudaStreamSynchronize(side);
+            cudaStreamDestroy(side);
+        }
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
         if (own_stream) {
             cudaStreamSynchronize(own_stream);
             cudaStreamDestroy(own_stream);
@@ -488,6 +515,7 @@ template <class R, class RN> class Solver final : public SolverBase {
         // a stream of its own: the legacy default stream cannot be captured into a graph
         CK(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
         stream = own_stream;
+        ensure_side();  // before any capture: stream creation is kept out of graphs
         nscene = ns;
         precision = p[0].precision;
         counts.assign(cnts, cnts + ns);
@@ -928,9 +956,22 @@ template <class R, class RN> class Solver final : public SolverBase {
 
     // the end of a step: the next step's first mirror generation at x^{n+1}, then the bucket
     // builds of x^{n+1} and of those mirrors
+    // The generation reads t_pos, t_prs, t_typ, the pre-build S.pid, the walls and the near
+    // flags and writes the raw mirrors; the fluid build reads the same t_* and S arrays and
+    // writes S2, its start tables, posf and its own key/rank scratch. Neither writes what the
+    // other reads, so with overlap_on the build runs on the second stream beside the
+    // generation and its cull, and the mirror bucket build (which reuses the key/rank
+    // scratch) waits for both. Both launches are issued before the build swaps S and S2 on
+    // the host, so the generation's arguments name the pre-build arrays either way.
     void step_tail() {
         const int bg = blk[MPS_K_GEN];
+        const bool fork = overlap_on && !timing_on;
         reset_raw();
+        if (fork) {
+            ensure_side();
+            CK(cudaEventRecord(ev_fork, stream));
+            CK(cudaStreamWaitEvent(side, ev_fork, 0));
+        }
         {
             Scope t(this, MPS_K_GEN);
             k_gen_cull<R, RN, false><<<blocks(nF, bg), bg, 0, stream>>>(args(M2, mcs2), t_pos,
@@ -938,7 +979,16 @@ template <class R, class RN> class Solver final : public SolverBase {
             KL();
             cull_raw();
         }
-        bin_fluid(t_pos, t_vel, nullptr, t_prs, S.pav, S.pid, t_typ);
+        if (fork) {
+            {
+                OnStream o(this, side);
+                bin_fluid(t_pos, t_vel, nullptr, t_prs, S.pav, S.pid, t_typ);
+                CK(cudaEventRecord(ev_join, side));
+            }
+            CK(cudaStreamWaitEvent(stream, ev_join, 0));
+        } else {
+            bin_fluid(t_pos, t_vel, nullptr, t_prs, S.pav, S.pid, t_typ);
+        }
         bin_mirrors(M1, mcs1);
     }
 

@@ -169,10 +169,12 @@ enum {
                                 (walking global memory) at their alternate register bound
                                 per thread (more or fewer resident blocks per SM; 0 = all
                                 at the default). Results never depend on it.              */
-    MPS_OPT_OVERLAP = 11     /* 1 (default): at the end of a step, the fluid bucket build
-                                runs on a second stream of the handle beside the next
-                                step's mirror generation (they share no array that either
-                                writes); 0: one stream. Steps timed with MPS_OPT_TIMING
+    MPS_OPT_OVERLAP = 11     /* work on a second stream of the handle, bit 0: at the end
+                                of a step the fluid bucket build beside the next step's
+                                mirror generation; bit 1: the step's second mirror
+                                generation (positions, cull, buckets) beside ChkCol/MkPrs,
+                                its pressures filled in after them. 3 (both) is the
+                                default, 0 one stream. Steps timed with MPS_OPT_TIMING
                                 always use one stream. Results never depend on it.       */
 };
 
@@ -266,9 +268,9 @@ int mps_create_batch(int32_t nscenes, const mps_params* p, const int32_t* counts
 
 int mps_destroy(mps_handle* h);
 /* Queue the handle's work on `cuda_stream` (a cudaStream_t); NULL selects the handle's own
- * non-blocking stream, which is the default. With MPS_OPT_OVERLAP the end of a step also
- * uses a second stream of the handle, forked from and joined back into this one, so work
- * queued on this stream after a step still runs after all of it. */
+ * non-blocking stream, which is the default. With MPS_OPT_OVERLAP a step also uses a
+ * second stream of the handle, forked from and joined back into this one, so work queued on
+ * this stream after a step still runs after all of it. */
 int mps_set_stream(mps_handle* h, void* cuda_stream);
 int mps_set_option(mps_handle* h, int32_t option, int32_t value);
 int mps_synchronize(mps_handle* h);

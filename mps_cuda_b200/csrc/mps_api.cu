@@ -209,7 +209,8 @@ int mps_set_option(mps_handle* h, int32_t opt, int32_t value) {
                 s.invalidate_graph();
                 break;
             case MPS_OPT_OVERLAP:
-                s.overlap_on = value != 0;
+                if (value < 0 || value > 3) throw ApiError(MPS_ERR_ARG, "overlap must lie in [0, 3]");
+                s.overlap = value;
                 s.invalidate_graph();
                 break;
             case MPS_OPT_STAGE_CAPACITY:
@@ -244,7 +245,7 @@ int mps_get_option(mps_handle* h, int32_t opt, int32_t* value) {
             case MPS_OPT_STAGE_CAPACITY: *value = s.stage_cap; break;
             case MPS_OPT_CANDIDATE_BATCH: *value = s.batch_a; break;
             case MPS_OPT_REGISTER_BOUND: *value = s.reg_bound; break;
-            case MPS_OPT_OVERLAP: *value = s.overlap_on; break;
+            case MPS_OPT_OVERLAP: *value = s.overlap; break;
             default: throw ApiError(MPS_ERR_ARG, "unknown option");
         }
     });

@@ -1496,7 +1496,9 @@ __device__ __forceinline__ void gen_reserve_emit(const PassArgs<R, RN>& a, const
 // GenMRR_nonslip + MRRinout for every FLD slot of (gpos, gprs, gtyp): the second generation
 // of a step (x*, P after pass B) and the first generation of the next one (x^{n+1}, P after
 // pass C). Near-wall particles are a thin layer, so this runs as a light kernel of its own
-// instead of stretching the neighbour passes.
+// instead of stretching the neighbour passes. With gprs null a mirror's pressure field holds
+// its owner's slot instead, for k_mirror_prs to replace once the pressures exist: the
+// positions of the second generation need only x*, so they are made beside pass B.
 template <class R, class RN, bool DIAG, bool TAPE = false>
 __global__ void __launch_bounds__(128, min_blocks<R>(10)) k_gen_cull(const __grid_constant__ PassArgs<R, RN> a, const V4<R>* gpos,
                                                   const R* gprs, const int8_t* gtyp) {
@@ -1519,11 +1521,25 @@ __global__ void __launch_bounds__(128, min_blocks<R>(10)) k_gen_cull(const __gri
             RowCtx<R> c = row_ctx(sc, p.x, p.y, p.z, ix, iy, iz);
             nw = plan_mirrors(sc, c, p.x, p.y, p.z, a.wl, a.skip != 0, pl);
             m = count_mirrors<R, RN>(pl, p.x, p.y, p.z, a.wl, a.cnt);
-            P = gprs[s];
+            P = gprs ? gprs[s] : slot_w(s, R(0));
         }
         if (DIAG) a.diag[size_t(pid) * kDiagCols + DG_GEN_W] = nw;
     }
     gen_reserve_emit<R, RN, TAPE>(a, pl, m, p.x, p.y, p.z, P, pid * kNumMRR);
+}
+
+// The pressures of a mirror generation made without them (k_gen_cull with gprs null), once
+// they exist: each bucketed mirror's owner slot, kept in its pressure field, becomes that
+// slot's pressure (PrsM = Prs of the owner, as the generation writes it directly). Only the
+// mirrors of the table's live buckets are read; a slot outside [0, nF) is left alone.
+template <class R>
+__global__ void k_mirror_prs(const int* __restrict__ mcs, int dead, V4<R>* __restrict__ mpos,
+                             const R* __restrict__ prs, int nF) {
+    const int n = __ldg(mcs + dead);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int s = w_slot(mpos[k].w);
+        if (s >= 0 && s < nF) mpos[k].w = prs[s];
+    }
 }
 
 // ---------------------------------------------------------------------------------------

@@ -274,7 +274,7 @@ struct SolverBase {
     int stage_cap = 0;                  // candidates staged per block (MPS_OPT_STAGE_CAPACITY)
     int batch_a = 4;                    // VscTrm's candidates in flight (MPS_OPT_CANDIDATE_BATCH)
     int reg_bound = 0;                  // passes B, C, A at their alternate register bound (bits 0-2)
-    bool overlap_on = true;             // the end of a step on two streams (MPS_OPT_OVERLAP)
+    int overlap = 3;                    // work on a second stream (MPS_OPT_OVERLAP bits 0-1)
     long long steps = 0;
     long long launches = 0;       // kernels launched (graph replays included)
     long long head_launches = 0;  // kernels of one captured step up to PrsGrdTrm
@@ -403,9 +403,10 @@ template <class R, class RN> class Solver final : public SolverBase {
     // slot order of S. It runs when the next step starts or when something reads the sorted
     // state, so a state replaced in between (mps_set_state) wastes no build.
     bool tail_pending = false;
-    // the second stream of a step's end (overlap_on), created at its first use, at the
-    // device's highest priority so that the bucket build's short scan launches get SMs while
-    // the mirror generation's blocks are pending; the fork and join events
+    // the handle's second stream (MPS_OPT_OVERLAP), created with the handle, at the device's
+    // highest priority: the work forked to it (the step end's fluid bucket build, the second
+    // mirror generation) gets SMs while the main stream's long kernel has blocks pending;
+    // the fork and join events
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     void ensure_side() {
@@ -919,7 +920,29 @@ template <class R, class RN> class Solver final : public SolverBase {
         }
         // MkBkt on x* (kernel.cu:1917); the rebuild at kernel.cu:1921 would give the same lists
         bin_fluid(t_pos, t_vel, nullptr, S.prs, S.pav, S.pid, t_typ);
-        // pass B: ChkCol + MkPrs, then the second mirror generation at (x*, P)
+        // The step's second mirror generation (the one the reference's counters would show
+        // last) is made at (x*, P): its positions, cull and bucket build need only x*, which
+        // ChkCol does not move (it changes velocities only, kernel.cu:1281-1287), and read
+        // nothing pass B writes; pass B reads the first generation's table M1, not the raw
+        // list, M2 or their scratch. So with bit 1 of overlap they run on the second stream
+        // beside pass B, and k_mirror_prs fills in the pressures once pass B has made them.
+        const bool fork = (overlap & 2) && !timing_on;
+        if (fork) {
+            CK(cudaEventRecord(ev_fork, stream));
+            CK(cudaStreamWaitEvent(side, ev_fork, 0));
+            OnStream o(this, side);
+            reset_raw();
+            {
+                Scope t(this, MPS_K_GEN);
+                k_gen_cull<R, RN, D><<<blocks(nF, bg), bg, 0, stream>>>(args(M1, mcs1), S.pos,
+                                                                               nullptr, S.typ);
+                KL();
+                cull_raw();
+            }
+            bin_mirrors(M2, mcs2);
+            CK(cudaEventRecord(ev_join, side));
+        }
+        // pass B: ChkCol + MkPrs
         {
             Scope t(this, MPS_K_PASS_B);
             if (reg_bound & 1)
@@ -928,16 +951,22 @@ template <class R, class RN> class Solver final : public SolverBase {
                 k_pass_b<R, RN, D><<<blocks(nF, bb), bb, 0, stream>>>(args(M1, mcs1));
             KL();
         }
-        reset_raw();
-        {
-            Scope t(this, MPS_K_GEN);
-            // the step's second generation: the one the reference's counters would show last
-            k_gen_cull<R, RN, D><<<blocks(nF, bg), bg, 0, stream>>>(args(M1, mcs1), S.pos,
-                                                                           t_prs, S.typ);
+        if (fork) {
+            CK(cudaStreamWaitEvent(stream, ev_join, 0));
+            k_mirror_prs<R><<<std::min(blocks(std::max(cap, 1), 256), 148 * 8), 256, 0, stream>>>(
+                mcs2, dead(), M2.pos, t_prs, nF);
             KL();
-            cull_raw();
+        } else {
+            reset_raw();
+            {
+                Scope t(this, MPS_K_GEN);
+                k_gen_cull<R, RN, D><<<blocks(nF, bg), bg, 0, stream>>>(args(M1, mcs1), S.pos,
+                                                                               t_prs, S.typ);
+                KL();
+                cull_raw();
+            }
+            bin_mirrors(M2, mcs2);
         }
-        bin_mirrors(M2, mcs2);
         // pass C: PrsGrdTrm + UpPcl2, then the first mirror generation of the next step
         {
             Scope t(this, MPS_K_PASS_C);
@@ -965,7 +994,7 @@ template <class R, class RN> class Solver final : public SolverBase {
     // the host, so the generation's arguments name the pre-build arrays either way.
     void step_tail() {
         const int bg = blk[MPS_K_GEN];
-        const bool fork = overlap_on && !timing_on;
+        const bool fork = (overlap & 1) && !timing_on;
         reset_raw();
         if (fork) {
             ensure_side();

@@ -179,7 +179,7 @@ def test_autotune_changes_no_result(prec):
     """Tuning tries every candidate of every knob (VscTrm's staging mode, candidate batch and
     block size, the other passes' block sizes and register bounds) on the handle's own state and restores it: the steps after
     it equal the oracle's. Then each knob is forced to every value it can take, and the
-    result is still the oracle's; last, the end of a step on one stream and on two."""
+    result is still the oracle's; last, each way of using the second stream."""
     g, o, _, _ = _pair("dambreak_l0.02_6k", prec, diag=False)
     g.step(2)
     chosen = g.autotune(2)
@@ -211,8 +211,8 @@ def test_autotune_changes_no_result(prec):
         g.step(1)
         o.step(1)
         _assert_same_state(g.state(), o.state(), ("register bound", rb))
-    # the end of a step on one stream, then again on two (the default)
-    for ov in (0, 1):
+    # one stream; the step end on two; the second mirror generation beside pass B; both
+    for ov in (0, 1, 2, 3):
         g.set_option(L.OPT_OVERLAP, ov)
         assert g.get_option(L.OPT_OVERLAP) == ov
         g.step(2)

@@ -5,8 +5,9 @@ allocate after start-up, plug-ins that only get input and output buffers -- call
 point with their own device buffers; its temporaries live in a fixed array inside the
 library. The test checks its output through the C-ABI against the solver's own bucket build
 (the bucket index mps_get_diag reports after MkBkt, and the order and start table that index
-implies), on two calls in a row, the second on a moved state while the fixed array still
-holds the first call's contents. The comparison is exact: the outputs are integers.
+implies) and against the oracle's MkBkt on the same positions, on two calls in a row, the
+second on a moved state while the fixed array still holds the first call's contents. The
+comparison is exact: the outputs are integers.
 
 This file is named to be collected last, so that a run stopping at the first failure has
 already run every other test.
@@ -20,6 +21,7 @@ import pytest
 
 from mps_cuda_b200 import F32, MPS, configs, dambreak, dambreak_params, derive, select_device
 from mps_cuda_b200 import _lib as L
+from oracle.oracle import Oracle, params_from
 
 pytestmark = pytest.mark.gpu
 
@@ -46,11 +48,16 @@ def test_noalloc_bucket_build_matches_solver():
     p = dambreak_params(desc, dt=dt, precision=F32)
     g = MPS(p, sc["typ"], sc["pos"].astype(np.float32), sc["vel"].astype(np.float32),
             sc["nrm"].astype(np.float32))
+    o = Oracle(params_from(p), sc["typ"], sc["pos"].astype(np.float32),
+               sc["vel"].astype(np.float32), sc["nrm"].astype(np.float32))
     n = g.n
     nb = derive(p).nbxyz
     for call in range(2):
         st = g.state()
         want = g.diag()["cell"]  # the solver's bucket index of every particle, -1 for GST
+        o.set_state(typ=st["typ"], pos=st["pos"])
+        o.phase(L.PHASE_MKBKT)  # the oracle's MkBkt (kernel.cu:516-550) on the same positions
+        assert np.array_equal(o.diag()["cell"], want), call
         typ_d = torch.from_numpy(st["typ"].copy()).cuda()
         pos_d = torch.from_numpy(np.ascontiguousarray(st["pos"])).cuda()
         rc, cell, order, start = _noalloc(torch, p, typ_d, pos_d, n, nb)
@@ -63,6 +70,7 @@ def test_noalloc_bucket_build_matches_solver():
         assert np.array_equal(start, expect_start), call
         g.step(5)  # move the particles before the second call
     g.close()
+    o.close()
 
 
 def test_noalloc_rejects_sizes_beyond_its_array():

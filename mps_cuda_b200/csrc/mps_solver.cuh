@@ -1703,6 +1703,21 @@ template <class R, class RN> class Solver final : public SolverBase {
         KL();
         bin_fluid(t_pos, t_vel, nullptr, S.prs, S.pav, S.pid, t_typ);
         a = tape_args(t.m1pos, t.m1slot, t.mcs1, t.nbB, t.nB, nullptr);
+        // the second mirror generation beside pass B, as in fused_body (overlap bit 1); the
+        // recorded copies after pass B read only arrays the generation reads too
+        const bool fork = (overlap & 2) && !timing_on;
+        if (fork) {
+            CK(cudaEventRecord(ev_fork, stream));
+            CK(cudaStreamWaitEvent(side, ev_fork, 0));
+            OnStream o(this, side);
+            reset_raw();
+            k_gen_cull<R, RN, false, true><<<blocks(nF, bg), bg, 0, stream>>>(a, S.pos, nullptr,
+                                                                                    S.typ);
+            KL();
+            cull_raw();
+            bin_mirrors_n(t.m2pos, t.m2slot, t.m2nrm, t.mcs2);
+            CK(cudaEventRecord(ev_join, side));
+        }
         k_pass_b<R, RN, false><<<blocks(nF, bb), bb, 0, stream>>>(a);
         KL();
         cp(t.pid2, S.pid, sizeof(int) * F);
@@ -1710,12 +1725,19 @@ template <class R, class RN> class Solver final : public SolverBase {
         cp(t.u2, S.vel, sizeof(V4<R>) * F);
         cp(t.vv2, t_vel, sizeof(V4<R>) * F);
         cp(t.P2, t_prs, sizeof(R) * F);
-        reset_raw();
-        k_gen_cull<R, RN, false, true><<<blocks(nF, bg), bg, 0, stream>>>(a, S.pos, t_prs,
-                                                                                S.typ);
-        KL();
-        cull_raw();
-        bin_mirrors_n(t.m2pos, t.m2slot, t.m2nrm, t.mcs2);
+        if (fork) {
+            CK(cudaStreamWaitEvent(stream, ev_join, 0));
+            k_mirror_prs<R><<<std::min(blocks(std::max(cap, 1), 256), 148 * 8), 256, 0, stream>>>(
+                t.mcs2, dead(), t.m2pos, t_prs, nF);
+            KL();
+        } else {
+            reset_raw();
+            k_gen_cull<R, RN, false, true><<<blocks(nF, bg), bg, 0, stream>>>(a, S.pos, t_prs,
+                                                                                    S.typ);
+            KL();
+            cull_raw();
+            bin_mirrors_n(t.m2pos, t.m2slot, t.m2nrm, t.mcs2);
+        }
         a = tape_args(t.m2pos, t.m2slot, t.mcs2, t.nbB, t.nB, t.vp2);
         k_pass_c<R, RN, false, true><<<blocks(nF, bc), bc, 0, stream>>>(a);
         KL();

@@ -100,6 +100,22 @@ def pair_arith(work: dict, diag: dict) -> dict:
     }
 
 
+NOMINAL_HBM_GBS = 8000.0  # B200 HBM3e, nominal (the measured copy bandwidth is the graded peak)
+
+
+def step_roofline(groups: dict, steps: int, ms_per_step: float, peak_gbs: float) -> dict:
+    """The whole step against HBM: the algorithmic bytes of every kernel group launched in
+    `steps` timed steps (the table above, per launch, times its launches), per step, over the
+    graph-replayed step time; as a fraction of the measured copy bandwidth and of the
+    nominal 8 TB/s."""
+    per_step = sum(v["alg_bytes"] * v["launches"] for v in groups.values()) / steps
+    ach = per_step / (ms_per_step / 1e3) / 1e9
+    return {"alg_bytes_per_step": per_step, "achieved": ach, "unit": "GB/s",
+            "frac": ach / peak_gbs, "frac_nominal": ach / NOMINAL_HBM_GBS,
+            "nominal_peak": NOMINAL_HBM_GBS,
+            "floor_ms_per_step": per_step / (peak_gbs * 1e9) * 1e3}
+
+
 def compute_roofline(ops, ms: float, ar: dict, f64: bool) -> dict:
     """Bound of one launch by the measured arithmetic rates: its flops at the fused
     multiply-add rate plus its square roots and divisions at theirs (they share the
@@ -539,6 +555,7 @@ def run_ours(args, world, rank, local):
             "clocks": clk.summary(), "wall_ms_per_step": 1e3 * wall / K,
             "e2e": e2e, "gpu_launches": launches,
             "roofline": roofline, "compute_roofline": compute, "kernel_groups": groups,
+            "step_roofline": step_roofline(groups, K, dev_ms_max / K, peak),
             "cpu_baseline": cpu,
             "batched": batched,
             "adjoint": adjoint,

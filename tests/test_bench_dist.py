@@ -138,3 +138,21 @@ print(json.dumps({'pkg': 'mps_cuda_b200' in sys.modules, 'so': 'libmps_b200' in 
     assert line["config"] == bench.bench_config("dambreak_l0.02_small", "f32",
                                                 int((typ == 0).sum()), int((typ != 0).sum()), 1)
     assert line["steps"] == 2 and line["warmup"] == 1
+
+
+def test_step_roofline_sums_the_groups_per_step():
+    """The whole-step HBM figure: every group's algorithmic bytes per launch times its
+    launches, per timed step, over the step time; against the measured and the nominal peak."""
+    import bench
+    s, nf, m1, m2, K = 4, 1000, 100, 120, 5
+    launches = {"pass_a": K, "pass_b": K, "pass_c": K, "gen_cull": 2 * K - 1,
+                "bin_fluid": 2 * K, "bin_mirror": 2 * K}
+    groups = {g: {"alg_bytes": bench.alg_bytes(g, s, nf, m1, m2), "launches": n}
+              for g, n in launches.items()}
+    r = bench.step_roofline(groups, K, 2.0, 5000.0)
+    per_step = sum(bench.alg_bytes(g, s, nf, m1, m2) * n for g, n in launches.items()) / K
+    assert r["alg_bytes_per_step"] == per_step
+    assert abs(r["achieved"] - per_step / 2e-3 / 1e9) < 1e-9 * r["achieved"]
+    assert abs(r["frac"] * 5000.0 - r["achieved"]) < 1e-9 * r["achieved"]
+    assert abs(r["frac_nominal"] * 8000.0 - r["achieved"]) < 1e-9 * r["achieved"]
+    assert abs(r["floor_ms_per_step"] - per_step / 5e12 * 1e3) < 1e-12
